@@ -1,0 +1,250 @@
+"""Python host binding of the B200 Burgers time step (``libbastr_gpu.so``, C ABI in
+``include/bastr_gpu.h``).
+
+``BastrGPU`` mirrors what the reference's Fortran driver does around the hot path:
+``readinput`` parameters in, ``set_state`` for ``read_initial_field`` plus the initial dealias
+of ``mainloop`` (solution.F90:41-52), ``step`` for iterations of the main loop
+(solution.F90:54-97), ``get_state`` for the fields ``writeflfed`` dumps, and ``mainloop`` for
+the whole loop with the reference's log lines.  Errors raise ``BastrError`` carrying the
+library's message, like the reference's ``stop 'message'``.
+
+There is no CPU fallback: constructing a solver without the built library or without a CUDA
+device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from .initfield import seeded_field  # noqa: F401  (re-export)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbastr_gpu.so")
+
+BASTR_OK = 0
+BASTR_E_INVALID = -1
+BASTR_E_UNSUPPORTED = -2
+BASTR_E_CUDA = -3
+BASTR_E_NAN = -4
+BASTR_E_STATE = -5
+BASTR_FP64 = 0
+BASTR_FP32 = 1
+
+EXPORTED = [
+    "bastr_create", "bastr_destroy", "bastr_set_state", "bastr_get_state", "bastr_set_counters",
+    "bastr_get_counters", "bastr_step", "bastr_step_async", "bastr_step_records", "bastr_spectra",
+    "bastr_fft", "bastr_set_stream", "bastr_sync", "bastr_info", "bastr_last_error",
+]
+
+
+class BastrError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"bastr error {code}: {msg}")
+        self.code = code
+
+
+class CParams(C.Structure):
+    _fields_ = [
+        ("ia", C.c_int32), ("ja", C.c_int32), ("ka", C.c_int32),
+        ("ref_tem", C.c_double), ("reynolds", C.c_double), ("deltat", C.c_double),
+        ("kmax", C.c_int32), ("timemethod", C.c_int32), ("forcemethod", C.c_int32),
+        ("forcek", C.c_int32), ("target_energy", C.c_double), ("lprojectd", C.c_int32),
+        ("precision", C.c_int32), ("device", C.c_int32), ("velgrad_every", C.c_int32),
+    ]
+
+
+class CStepOut(C.Structure):
+    _fields_ = [
+        ("nstep", C.c_int64), ("time", C.c_double),
+        ("Esspe", C.c_double), ("Edspe", C.c_double), ("k2Edspe", C.c_double), ("kMEdspe", C.c_double),
+        ("velgrad", C.c_double * 8), ("factor", C.c_double), ("E", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the CUDA library; raises if it has not been built (no fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: run `python -m bastr_b200.build`")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    lib.bastr_create.argtypes = [C.POINTER(CParams), C.POINTER(P)]
+    lib.bastr_destroy.argtypes = [P]
+    lib.bastr_set_state.argtypes = [P, D, D, D]
+    lib.bastr_get_state.argtypes = [P, D, D, D]
+    lib.bastr_set_counters.argtypes = [P, C.c_int64, C.c_double]
+    lib.bastr_get_counters.argtypes = [P, C.POINTER(C.c_int64), D]
+    lib.bastr_step.argtypes = [P, C.c_int32, C.POINTER(CStepOut), D]
+    lib.bastr_step_async.argtypes = [P, C.c_int32]
+    lib.bastr_step_records.argtypes = [P, C.c_int32, C.POINTER(CStepOut), D]
+    lib.bastr_spectra.argtypes = [P, D, D, D, C.POINTER(C.c_int64)]
+    lib.bastr_fft.argtypes = [P, D, C.c_int32]
+    lib.bastr_set_stream.argtypes = [P, P]
+    lib.bastr_sync.argtypes = [P]
+    lib.bastr_info.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    lib.bastr_last_error.argtypes = [P, C.c_char_p, C.c_int32]
+    for name in EXPORTED:
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+@dataclass
+class StepRecord:
+    nstep: int
+    time: float
+    Esspe: float
+    Edspe: float
+    k2Edspe: float
+    kMEdspe: float
+    velgrad: tuple
+    factor: float
+    E: float
+
+
+def miucal(temper: float, ref_tem: float) -> float:
+    """Sutherland viscosity law (solution.F90:1315-1329)."""
+    tc = 110.4 / ref_tem
+    return temper * math.sqrt(temper) * (1.0 + tc) / (temper + tc)
+
+
+class BastrGPU:
+    """One solver handle on one GPU (see module docstring)."""
+
+    def __init__(self, ia: int, ja: int, ka: int = 0, *, ref_tem: float = 273.15,
+                 reynolds: float = 5000.0, deltat: float = 1e-4, kmax: int = 1 << 30,
+                 timemethod: int = 1, forcemethod: int = 0, forcek: int = 5,
+                 target_energy: float = 0.075, lprojectd: bool = False,
+                 precision: str = "fp64", device: int = 0, velgrad_every: int = 1):
+        self.lib = load_library()
+        p = CParams(ia, ja, ka, ref_tem, reynolds, deltat, kmax, timemethod, forcemethod, forcek,
+                    target_energy, 1 if lprojectd else 0,
+                    BASTR_FP32 if precision == "fp32" else BASTR_FP64, device, velgrad_every)
+        self._p = p
+        self.h = C.c_void_p()
+        rc = self.lib.bastr_create(C.byref(p), C.byref(self.h))
+        if rc != BASTR_OK:
+            msg = self._err()
+            self.close()
+            raise BastrError(rc, msg)
+        self.ndims = 2 if ka == 0 else 3
+        self.shape = (ja, ia) if ka == 0 else (ka, ja, ia)
+        self.deltat = deltat
+        self.forcemethod = forcemethod
+        a = C.c_int32()
+        self.lib.bastr_info(self.h, C.byref(a), None, None)
+        self.allkmax = a.value
+
+    # -- plumbing ------------------------------------------------------------------------
+    def _err(self) -> str:
+        buf = C.create_string_buffer(1024)
+        if self.h:
+            self.lib.bastr_last_error(self.h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc: int):
+        if rc != BASTR_OK:
+            raise BastrError(rc, self._err())
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.bastr_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        a, n, b = C.c_int32(), C.c_int32(), C.c_int64()
+        self._check(self.lib.bastr_info(self.h, C.byref(a), C.byref(n), C.byref(b)))
+        return {"allkmax": a.value, "launches_per_step": n.value, "device_bytes": b.value}
+
+    # -- state ---------------------------------------------------------------------------
+    def set_state(self, u):
+        arrs = [np.ascontiguousarray(c, dtype=np.float64).reshape(self.shape) for c in u]
+        if len(arrs) != self.ndims:
+            raise ValueError("one array per velocity component")
+        u3 = arrs[2] if self.ndims == 3 else arrs[0]
+        self._check(self.lib.bastr_set_state(self.h, _dptr(arrs[0]), _dptr(arrs[1]), _dptr(u3)))
+
+    def get_state(self):
+        out = [np.empty(self.shape, dtype=np.float64) for _ in range(self.ndims)]
+        u3 = out[2] if self.ndims == 3 else out[0]
+        self._check(self.lib.bastr_get_state(self.h, _dptr(out[0]), _dptr(out[1]), _dptr(u3)))
+        return out
+
+    def set_counters(self, nstep: int, time: float):
+        self._check(self.lib.bastr_set_counters(self.h, nstep, time))
+
+    def counters(self):
+        n, t = C.c_int64(), C.c_double()
+        self._check(self.lib.bastr_get_counters(self.h, C.byref(n), C.byref(t)))
+        return n.value, t.value
+
+    # -- stepping ------------------------------------------------------------------------
+    @staticmethod
+    def _rec(o: CStepOut) -> StepRecord:
+        return StepRecord(o.nstep, o.time, o.Esspe, o.Edspe, o.k2Edspe, o.kMEdspe,
+                          tuple(o.velgrad), o.factor, o.E)
+
+    def step(self, nsteps: int = 1, shells: bool = False):
+        """Runs nsteps main-loop iterations; returns records (and per-step Es/Ed shells)."""
+        out = (CStepOut * max(nsteps, 1))()
+        sh = np.empty((max(nsteps, 1), 2, self.allkmax + 1), dtype=np.float64) if shells else None
+        rc = self.lib.bastr_step(self.h, nsteps, out, _dptr(sh) if sh is not None else None)
+        recs = [self._rec(out[i]) for i in range(nsteps)]
+        if rc != BASTR_OK:
+            raise BastrError(rc, self._err())
+        return (recs, sh[:nsteps]) if shells else recs
+
+    def step_async(self, nsteps: int):
+        self._check(self.lib.bastr_step_async(self.h, nsteps))
+
+    def records(self, nsteps: int):
+        out = (CStepOut * max(nsteps, 1))()
+        self._check(self.lib.bastr_step_records(self.h, nsteps, out, None))
+        return [self._rec(out[i]) for i in range(nsteps)]
+
+    def sync(self):
+        self._check(self.lib.bastr_sync(self.h))
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.lib.bastr_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def spectra(self):
+        n = self.allkmax + 1
+        kn, es, ed = (np.empty(n) for _ in range(3))
+        ec = np.empty(n, dtype=np.int64)
+        self._check(self.lib.bastr_spectra(self.h, _dptr(kn), _dptr(es), _dptr(ed),
+                                           ec.ctypes.data_as(C.POINTER(C.c_int64))))
+        return kn, es, ed, ec
+
+    def fft(self, array: np.ndarray, direction: int) -> np.ndarray:
+        """fft2d/fft3d (direction -1, scaled 1/N) or ifft2d/ifft3d (+1) of a full complex grid."""
+        a = np.ascontiguousarray(array, dtype=np.complex128).reshape(self.shape).copy()
+        self._check(self.lib.bastr_fft(self.h, a.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
+                                       direction))
+        return a

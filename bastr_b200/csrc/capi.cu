@@ -1,0 +1,837 @@
+// C ABI of the B200 Burgers time step: handle, device buffers, launch schedule.
+//
+// One translation unit: the pass kernels are included so that every template instance the
+// schedule needs is generated here.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/bastr_gpu.h"
+#include "diag.cu"
+#include "pass2d.cu"
+#include "pass3d.cu"
+
+using namespace bastr;
+
+namespace {
+
+constexpr int kChunk = 256;   // records kept on the device per batch chunk
+
+struct Twiddles {
+    int n = 0;
+    double2* d64 = nullptr;
+    float2* d32 = nullptr;
+};
+
+}  // namespace
+
+struct bastr_handle {
+    bastr_params p{};
+    Geo g{};
+    int fp32 = 0;
+    int allkmax = 0;
+    int nshell = 0;            // shells 0..K cover every kept mode
+    int64_t nstep = 0;
+    double time = 0.0;
+    bool have_state = false;
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // device buffers
+    double2* u0 = nullptr;     // truncated state, FP64
+    void* us = nullptr;        // stage input (compute precision)
+    void* acc = nullptr;       // RK accumulator (compute precision)
+    void* ma = nullptr;        // mixed fields after the first inverse pass(es)
+    void* mb = nullptr;        // mixed fields before the last forward pass(es)
+    void* mc = nullptr;        // 3D only: second mixed buffer
+    double* phys = nullptr;    // physical fields for set/get (d * npts)
+    double* vg_part = nullptr;
+    double* en_part = nullptr;
+    double* shell = nullptr;   // [nshell][4]
+    double* rec = nullptr;     // [kChunk][R_COUNT]
+    double* shells_dev = nullptr; // [kChunk][2][allkmax+1]
+    int64_t dev_bytes = 0;
+    size_t n_state = 0;        // complex entries of the truncated state (all components)
+    int n_vg_blocks = 0;
+    int n_en_blocks = 0;
+    int launches_per_step = 0;
+    int chunk_used = 0;        // records written by the last async batch
+    int64_t batch_n0 = 0;      // nstep and time at the start of that batch
+    double batch_t0 = 0.0;
+    Twiddles tw[3];            // per axis x, y, z
+    std::vector<double> kn;
+    std::vector<int64_t> ecount;
+};
+
+namespace {
+
+int fail(bastr_handle* h, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(h, BASTR_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                              \
+    } while (0)
+
+bool is_pow2(int n) { return n >= 16 && n <= 2048 && (n & (n - 1)) == 0; }
+
+template <typename T> const cplx<T>* twp(const Twiddles& t);
+template <> const cplx<double>* twp<double>(const Twiddles& t) { return t.d64; }
+template <> const cplx<float>* twp<float>(const Twiddles& t) { return t.d32; }
+
+// Enables the dynamic shared memory a kernel instance asks for, once per (device, kernel).
+std::mutex g_prep_mu;
+std::set<std::pair<int, const void*>> g_prepped;
+template <typename K> cudaError_t prep(K kernel, size_t smem) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const auto key = std::make_pair(dev, (const void*)kernel);
+    std::lock_guard<std::mutex> lk(g_prep_mu);
+    if (g_prepped.count(key)) return cudaSuccess;
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    g_prepped.insert(key);
+    return cudaSuccess;
+}
+
+#define SIZE_CASES(N, ...)                      \
+    switch (N) {                                 \
+        case 16: { constexpr int NN = 16; __VA_ARGS__; } break;     \
+        case 32: { constexpr int NN = 32; __VA_ARGS__; } break;     \
+        case 64: { constexpr int NN = 64; __VA_ARGS__; } break;     \
+        case 128: { constexpr int NN = 128; __VA_ARGS__; } break;   \
+        case 256: { constexpr int NN = 256; __VA_ARGS__; } break;   \
+        case 512: { constexpr int NN = 512; __VA_ARGS__; } break;   \
+        case 1024: { constexpr int NN = 1024; __VA_ARGS__; } break; \
+        case 2048: { constexpr int NN = 2048; __VA_ARGS__; } break; \
+        default: return cudaErrorInvalidValue;   \
+    }
+
+// ---------------------------------------------------------------------------------------
+// 2D launches
+// ---------------------------------------------------------------------------------------
+template <typename T, typename TIN, int SET>
+cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
+    SIZE_CASES(h->g.ny, {
+        using P = YInv2D<T, NN, SET>;
+        auto k = k2d_yinv<T, TIN, NN, SET>;
+        cudaError_t e = prep(k, P::SMEM);
+        if (e != cudaSuccess) return e;
+        k<<<h->g.K, P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g,
+                                                  twp<T>(h->tw[1]));
+    });
+    return cudaGetLastError();
+}
+
+template <typename T, int MODE>
+cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const double* pin, double* pout,
+                     double* vg) {
+    SIZE_CASES(h->g.nx, {
+        using P = XPass2D<T, NN, MODE>;
+        auto k = k2d_xpass<T, NN, MODE>;
+        cudaError_t e = prep(k, P::SMEM);
+        if (e != cudaSuccess) return e;
+        k<<<h->g.ny / P::BR, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg,
+                                                          h->g, twp<T>(h->tw[0]));
+    });
+    return cudaGetLastError();
+}
+
+template <typename T, int EPI>
+cudaError_t l2_yfwd(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0) {
+    SIZE_CASES(h->g.ny, {
+        using P = YFwd2D<T, NN>;
+        auto k = k2d_yfwd<T, NN, EPI>;
+        cudaError_t e = prep(k, P::SMEM);
+        if (e != cudaSuccess) return e;
+        k<<<h->g.K, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]));
+    });
+    return cudaGetLastError();
+}
+
+template <typename T> int xpass_rows(bastr_handle* h, bool vg) {
+    (void)h;
+    return vg ? XPass2D<T, 64, XM_RHS_VG>::BR : XPass2D<T, 64, XM_RHS>::BR;
+}
+
+// One right-hand-side evaluation F(u_s) and its combination, 2D.
+template <typename T>
+cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
+    cudaError_t e;
+    const int ftot = vg ? 7 : 4;
+    if (from_u0) e = l2_yinv<T, double, YI_RHS>(h, h->u0, h->ma, ftot);
+    else e = l2_yinv<T, T, YI_RHS>(h, h->us, h->ma, ftot);
+    if (e != cudaSuccess) return e;
+    if (vg) {
+        e = l2_yinv<T, double, YI_VG>(h, h->u0, h->ma, ftot);
+        if (e != cudaSuccess) return e;
+        e = l2_xpass<T, XM_RHS_VG>(h, h->ma, ftot, h->mb, nullptr, nullptr, h->vg_part);
+    } else {
+        e = l2_xpass<T, XM_RHS>(h, h->ma, ftot, h->mb, nullptr, nullptr, nullptr);
+    }
+    if (e != cudaSuccess) return e;
+    StageIO<T> io{h->u0, (cplx<T>*)h->us, (cplx<T>*)h->acc, nullptr};
+    const bool need_en = (epi == EPI_RK3 || epi == EPI_CN_LAST) &&
+                         (h->p.forcemethod == 1 || h->p.forcemethod == 5);
+    if (need_en) io.energy_part = h->en_part;
+    switch (epi) {
+        case EPI_RK1: return l2_yfwd<T, EPI_RK1>(h, h->mb, io, from_u0);
+        case EPI_RK2: return l2_yfwd<T, EPI_RK2>(h, h->mb, io, from_u0);
+        case EPI_RK3: return l2_yfwd<T, EPI_RK3>(h, h->mb, io, from_u0);
+        case EPI_CN_MID: return l2_yfwd<T, EPI_CN_MID>(h, h->mb, io, from_u0);
+        case EPI_CN_LAST: return l2_yfwd<T, EPI_CN_LAST>(h, h->mb, io, from_u0);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------------------
+// 3D launches
+// ---------------------------------------------------------------------------------------
+#define SIZE_CASES3(N, ...)                                  \
+    switch (N) {                                              \
+        case 16: { constexpr int NN = 16; __VA_ARGS__; } break;     \
+        case 32: { constexpr int NN = 32; __VA_ARGS__; } break;     \
+        case 64: { constexpr int NN = 64; __VA_ARGS__; } break;     \
+        case 128: { constexpr int NN = 128; __VA_ARGS__; } break;   \
+        case 256: { constexpr int NN = 256; __VA_ARGS__; } break;   \
+        case 512: { constexpr int NN = 512; __VA_ARGS__; } break;   \
+        default: return cudaErrorInvalidValue;                \
+    }
+
+int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+template <typename T, typename TIN, int SET>
+cudaError_t l3_zinv(bastr_handle* h, const void* S, void* MA, int ftot) {
+    SIZE_CASES3(h->g.nz, {
+        using P = ZInv3D<T, NN, SET>;
+        auto k = k3d_zinv<T, TIN, NN, SET>;
+        cudaError_t e = prep(k, P::SMEM);
+        if (e != cudaSuccess) return e;
+        k<<<cdiv(h->g.K * h->g.KY, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot,
+                                                                         h->g, twp<T>(h->tw[2]));
+    });
+    return cudaGetLastError();
+}
+
+template <typename T, int SET>
+cudaError_t l3_yinv(bastr_handle* h, const void* MA, void* MB) {
+    SIZE_CASES3(h->g.ny, {
+        using P = YInv3D<T, NN, SET>;
+        auto k = k3d_yinv<T, NN, SET>;
+        cudaError_t e = prep(k, P::SMEM);
+        if (e != cudaSuccess) return e;
+        k<<<cdiv(h->g.K * h->g.nz, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, (cplx<T>*)MB, h->g,
+                                                                         twp<T>(h->tw[1]));
+    });
+    return cudaGetLastError();
+}
+
+template <typename T, int MODE>
+cudaError_t l3_xpass(bastr_handle* h, const void* MB, void* MC, const double* pin, double* pout, double* vg) {
+    SIZE_CASES3(h->g.nx, {
+        using P = XPass3D<T, NN, MODE>;
+        auto k = k3d_xpass<T, NN, MODE>;
+        cudaError_t e = prep(k, P::SMEM);
+        if (e != cudaSuccess) return e;
+        k<<<h->g.ny * h->g.nz / P::BR, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg,
+                                                                       h->g, twp<T>(h->tw[0]));
+    });
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t l3_yfwd(bastr_handle* h, const void* MC, void* MD) {
+    SIZE_CASES3(h->g.ny, {
+        using P = YFwd3D<T, NN>;
+        auto k = k3d_yfwd<T, NN>;
+        cudaError_t e = prep(k, P::SMEM);
+        if (e != cudaSuccess) return e;
+        k<<<cdiv(h->g.K * h->g.nz, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MC, (cplx<T>*)MD, h->g,
+                                                                         twp<T>(h->tw[1]));
+    });
+    return cudaGetLastError();
+}
+
+template <typename T, int EPI>
+cudaError_t l3_zfwd(bastr_handle* h, const void* MD, StageIO<T> io, int from_u0) {
+    SIZE_CASES3(h->g.nz, {
+        using P = ZFwd3D<T, NN>;
+        auto k = k3d_zfwd<T, NN, EPI>;
+        cudaError_t e = prep(k, P::SMEM);
+        if (e != cudaSuccess) return e;
+        k<<<cdiv(h->g.K * h->g.KY, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MD, io, from_u0, h->g,
+                                                                         twp<T>(h->tw[2]));
+    });
+    return cudaGetLastError();
+}
+
+template <typename T> int zfwd_lines(int nz) {
+    switch (nz) {
+        case 16: return ZFwd3D<T, 16>::L;
+        case 32: return ZFwd3D<T, 32>::L;
+        case 64: return ZFwd3D<T, 64>::L;
+        case 128: return ZFwd3D<T, 128>::L;
+        case 256: return ZFwd3D<T, 256>::L;
+        default: return ZFwd3D<T, 512>::L;
+    }
+}
+template <typename T> int xpass3_rows_vg(int nx) {
+    switch (nx) {
+        case 16: return XPass3D<T, 16, X3_RHS_VG>::BR;
+        case 32: return XPass3D<T, 32, X3_RHS_VG>::BR;
+        case 64: return XPass3D<T, 64, X3_RHS_VG>::BR;
+        case 128: return XPass3D<T, 128, X3_RHS_VG>::BR;
+        case 256: return XPass3D<T, 256, X3_RHS_VG>::BR;
+        default: return XPass3D<T, 512, X3_RHS_VG>::BR;
+    }
+}
+
+int vg_blocks3d(bastr_handle* h) {
+    const int br = h->fp32 ? xpass3_rows_vg<float>(h->g.nx) : xpass3_rows_vg<double>(h->g.nx);
+    return h->g.ny * h->g.nz / br;
+}
+int en_blocks3d(bastr_handle* h) {
+    const int l = h->fp32 ? zfwd_lines<float>(h->g.nz) : zfwd_lines<double>(h->g.nz);
+    return cdiv(h->g.K * h->g.KY, l);
+}
+
+// Mixed-field buffer sizes (bytes) for compute element size cs.
+void sizes3d(bastr_handle* h, size_t cs, size_t& ma, size_t& mb, size_t& mc) {
+    const Geo& g = h->g;
+    const size_t K = g.K, KY = g.KY, NY = g.ny, NZ = g.nz;
+    const size_t c64 = sizeof(double2);
+    ma = std::max({K * NZ * KY * 10 * cs, K * KY * NZ * 3 * cs, K * NZ * KY * 3 * c64, K * KY * NZ * 3 * c64});
+    mb = std::max(NZ * NY * K * 13 * cs, NZ * NY * K * 3 * c64);
+    mc = std::max(NZ * K * NY * 3 * cs, NZ * K * NY * 3 * c64);
+}
+
+template <typename T>
+cudaError_t rhs3d(bastr_handle* h, int epi, bool from_u0, bool vg) {
+    cudaError_t e;
+    const int ftot = vg ? 10 : 6;
+    if (from_u0) e = l3_zinv<T, double, ZI_RHS>(h, h->u0, h->ma, ftot);
+    else e = l3_zinv<T, T, ZI_RHS>(h, h->us, h->ma, ftot);
+    if (e != cudaSuccess) return e;
+    if (vg) {
+        e = l3_zinv<T, double, ZI_VG>(h, h->u0, h->ma, ftot);
+        if (e != cudaSuccess) return e;
+        e = l3_yinv<T, YB_RHS_VG>(h, h->ma, h->mb);
+        if (e != cudaSuccess) return e;
+        e = l3_xpass<T, X3_RHS_VG>(h, h->mb, h->mc, nullptr, nullptr, h->vg_part);
+    } else {
+        e = l3_yinv<T, YB_RHS>(h, h->ma, h->mb);
+        if (e != cudaSuccess) return e;
+        e = l3_xpass<T, X3_RHS>(h, h->mb, h->mc, nullptr, nullptr, nullptr);
+    }
+    if (e != cudaSuccess) return e;
+    e = l3_yfwd<T>(h, h->mc, h->ma);
+    if (e != cudaSuccess) return e;
+    StageIO<T> io{h->u0, (cplx<T>*)h->us, (cplx<T>*)h->acc, nullptr};
+    const bool need_en = (epi == EPI_RK3 || epi == EPI_CN_LAST) &&
+                         (h->p.forcemethod == 1 || h->p.forcemethod == 5);
+    if (need_en) io.energy_part = h->en_part;
+    switch (epi) {
+        case EPI_RK1: return l3_zfwd<T, EPI_RK1>(h, h->ma, io, from_u0);
+        case EPI_RK2: return l3_zfwd<T, EPI_RK2>(h, h->ma, io, from_u0);
+        case EPI_RK3: return l3_zfwd<T, EPI_RK3>(h, h->ma, io, from_u0);
+        case EPI_CN_MID: return l3_zfwd<T, EPI_CN_MID>(h, h->ma, io, from_u0);
+        case EPI_CN_LAST: return l3_zfwd<T, EPI_CN_LAST>(h, h->ma, io, from_u0);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t state3d_to_spectral(bastr_handle* h) {
+    cudaError_t e = l3_xpass<double, X3_FROM_PHYS>(h, nullptr, h->mc, h->phys, nullptr, nullptr);
+    if (e != cudaSuccess) return e;
+    e = l3_yfwd<double>(h, h->mc, h->ma);
+    if (e != cudaSuccess) return e;
+    StageIO<double> io{h->u0, nullptr, nullptr, nullptr};
+    return l3_zfwd<double, EPI_STORE>(h, h->ma, io, 0);
+}
+
+cudaError_t state3d_to_physical(bastr_handle* h) {
+    cudaError_t e = l3_zinv<double, double, ZI_STATE>(h, h->u0, h->ma, 3);
+    if (e != cudaSuccess) return e;
+    e = l3_yinv<double, YB_STATE>(h, h->ma, h->mb);
+    if (e != cudaSuccess) return e;
+    return l3_xpass<double, X3_TO_PHYS>(h, h->mb, nullptr, nullptr, h->phys, nullptr);
+}
+
+int full_fft(bastr_handle* h, double* array, int dir) {
+    (void)array;
+    (void)dir;
+    return fail(h, BASTR_E_UNSUPPORTED, "bastr_fft is not built yet");
+}
+
+// ---------------------------------------------------------------------------------------
+// dimension-generic step pieces
+// ---------------------------------------------------------------------------------------
+cudaError_t launch_rhs(bastr_handle* h, int epi, bool from_u0, bool vg) {
+    if (h->g.d == 2) return h->fp32 ? rhs2d<float>(h, epi, from_u0, vg) : rhs2d<double>(h, epi, from_u0, vg);
+    return h->fp32 ? rhs3d<float>(h, epi, from_u0, vg) : rhs3d<double>(h, epi, from_u0, vg);
+}
+
+cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out) {
+    if (h->g.d == 2) k_spectra<2, 256><<<h->nshell, 256, 0, h->stream>>>(h->u0, h->g, h->shell);
+    else k_spectra<3, 256><<<h->nshell, 256, 0, h->stream>>>(h->u0, h->g, h->shell);
+    k_spectra_final<256><<<1, 256, 0, h->stream>>>(h->shell, h->nshell, h->allkmax, rec, shells_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forcing(bastr_handle* h, double* rec) {
+    const int m = h->p.forcemethod;
+    if (m == 0) return cudaSuccess;
+    if (m == 1 || m == 5) {
+        k_sum_partials<256><<<1, 256, 0, h->stream>>>(h->en_part, h->n_en_blocks, 1.0, rec, R_ENERGY);
+    }
+    if (m == 1) {
+        k_force_linear_factor<<<1, 32, 0, h->stream>>>(rec, h->p.target_energy);
+        k_scale_state<<<148 * 4, 256, 0, h->stream>>>(h->u0, h->n_state, rec);
+    } else {
+        const int proj = (m == 5 && h->g.d == 2 && h->p.lprojectd) ? 1 : 0;
+        if (h->g.d == 2)
+            k_force_band<2, 256><<<1, 256, 0, h->stream>>>(h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec);
+        else
+            k_force_band<3, 256><<<1, 256, 0, h->stream>>>(h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec);
+    }
+    return cudaGetLastError();
+}
+
+// One iteration of the main loop body for record slot `slot`.
+cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
+    double* rec = h->rec + (size_t)slot * R_COUNT;
+    double* sh = h->shells_dev + (size_t)slot * 2 * (h->allkmax + 1);
+    cudaError_t e = launch_spectra(h, rec, sh);
+    if (e != cudaSuccess) return e;
+    if (h->p.timemethod == 1) {
+        e = launch_rhs(h, EPI_RK1, true, vg);
+        if (e != cudaSuccess) return e;
+        if (vg) k_velgrad_final<256><<<1, 256, 0, h->stream>>>(h->vg_part, h->n_vg_blocks, h->g, rec);
+        e = launch_rhs(h, EPI_RK2, false, false);
+        if (e != cudaSuccess) return e;
+        e = launch_rhs(h, EPI_RK3, false, false);
+        if (e != cudaSuccess) return e;
+    } else {
+        for (int s = 1; s <= 6; ++s) {
+            e = launch_rhs(h, s == 6 ? EPI_CN_LAST : EPI_CN_MID, s == 1, vg && s == 1);
+            if (e != cudaSuccess) return e;
+            if (vg && s == 1) k_velgrad_final<256><<<1, 256, 0, h->stream>>>(h->vg_part, h->n_vg_blocks, h->g, rec);
+        }
+    }
+    return launch_forcing(h, rec);
+}
+
+int count_launches(bastr_handle* h, bool vg) {
+    int n = 2;                                      // spectra + final
+    const int per_rhs = h->g.d == 2 ? 3 : 5;
+    const int nrhs = h->p.timemethod == 1 ? 3 : 6;
+    n += per_rhs * nrhs;
+    if (vg) n += (h->g.d == 2 ? 1 : 1) + 1;         // extra inverse pass + final reduction
+    const int m = h->p.forcemethod;
+    if (m == 1) n += 3;
+    else if (m == 2) n += 1;
+    else if (m == 5) n += 2;
+    return n;
+}
+
+void host_twiddles(int n, std::vector<double2>& t64, std::vector<float2>& t32) {
+    t64.resize(n);
+    t32.resize(n);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < n; ++m) {
+        const long double a = -2.0L * pi * (long double)m / (long double)n;
+        const double c = (double)cosl(a), s = (double)sinl(a);
+        t64[m] = make_double2(c, s);
+        t32[m] = make_float2((float)cosl(a), (float)sinl(a));
+    }
+}
+
+// Shell geometry over the full grid: Ecount and kn (solution.F90:974-995).
+void host_shells(bastr_handle* h) {
+    const int am = h->allkmax;
+    std::vector<double> ksum(am + 1, 0.0);
+    std::vector<int64_t> cnt(am + 1, 0);
+    auto wav = [](int i, int n) { return i <= n / 2 ? i : i - n; };
+    const int nx = h->g.nx, ny = h->g.ny, nz = h->g.d == 3 ? h->g.nz : 1;
+    const double lim = (am + 0.5) * (am + 0.5);
+    for (int k = 0; k < nz; ++k) {
+        const int kz = h->g.d == 3 ? wav(k, nz) : 0;
+        for (int j = 0; j < ny; ++j) {
+            const int ky = wav(j, ny);
+            const double r2 = (double)ky * ky + (double)kz * kz;
+            if (r2 > lim) continue;
+            for (int i = 0; i < nx; ++i) {
+                const int kx = wav(i, nx);
+                const double m = r2 + (double)kx * kx;
+                if (m > lim) continue;
+                const double kk = std::sqrt(m);
+                const int s = (int)std::floor(kk / 1.0 + 0.5);
+                if (s <= am) {
+                    cnt[s] += 1;
+                    ksum[s] += kk;
+                }
+            }
+        }
+    }
+    h->kn.assign(am + 1, 0.0);
+    h->ecount = cnt;
+    h->kn[0] = ksum[0];
+    for (int s = 1; s <= am; ++s) h->kn[s] = ksum[s] / (double)cnt[s];
+}
+
+template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cudaError_t& st) {
+    if (st != cudaSuccess) return;
+    void* q = nullptr;
+    st = cudaMalloc(&q, bytes ? bytes : 16);
+    if (st == cudaSuccess) {
+        st = cudaMemset(q, 0, bytes ? bytes : 16);
+        h->dev_bytes += (int64_t)bytes;
+    }
+    *ptr = (P*)q;
+}
+
+void free_all(bastr_handle* h) {
+    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part,
+                    h->shell, h->rec, h->shells_dev};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    for (auto& t : h->tw) {
+        if (t.d64) cudaFree(t.d64);
+        if (t.d32) cudaFree(t.d32);
+    }
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+// Physical <-> truncated spectral state, always in FP64.
+cudaError_t to_spectral(bastr_handle* h) {
+    cudaError_t e;
+    if (h->g.d == 2) {
+        e = l2_xpass<double, XM_FROM_PHYS>(h, nullptr, 0, h->mb, h->phys, nullptr, nullptr);
+        if (e != cudaSuccess) return e;
+        StageIO<double> io{h->u0, nullptr, nullptr, nullptr};
+        return l2_yfwd<double, EPI_STORE>(h, h->mb, io, 0);
+    }
+    return state3d_to_spectral(h);
+}
+
+cudaError_t to_physical(bastr_handle* h) {
+    cudaError_t e;
+    if (h->g.d == 2) {
+        e = l2_yinv<double, double, YI_STATE>(h, h->u0, h->ma, 2);
+        if (e != cudaSuccess) return e;
+        return l2_xpass<double, XM_TO_PHYS>(h, h->ma, 2, nullptr, nullptr, h->phys, nullptr);
+    }
+    return state3d_to_physical(h);
+}
+
+}  // namespace
+
+// =========================================================================================
+// exported C ABI
+// =========================================================================================
+extern "C" {
+
+int bastr_create(const bastr_params* p, bastr_handle** out) {
+    if (!p || !out) return BASTR_E_INVALID;
+    *out = nullptr;
+    bastr_handle* h = new bastr_handle();
+    h->p = *p;
+    const int d = p->ka == 0 ? 2 : 3;
+    *out = h;   // also on failure, so that the caller can read the message; destroy it either way
+    if (p->ja == 0) return fail(h, BASTR_E_INVALID, "1D case is not implemented yet!");
+    if (p->timemethod != 1 && p->timemethod != 2) { int r = fail(h, BASTR_E_INVALID, "Undefined time method"); return r; }
+    if (p->forcemethod == 3 || p->forcemethod == 4) {
+        int r = fail(h, BASTR_E_UNSUPPORTED, "forcemethod %d (random-phase forcing) is not supported", p->forcemethod);
+        return r;
+    }
+    if (p->forcemethod < 0 || p->forcemethod > 5) { int r = fail(h, BASTR_E_INVALID, "forcemethod %d", p->forcemethod); return r; }
+    if (p->precision != BASTR_FP64 && p->precision != BASTR_FP32) { int r = fail(h, BASTR_E_INVALID, "precision"); return r; }
+    const int nz = d == 3 ? p->ka : 1;
+    if (!is_pow2(p->ia) || !is_pow2(p->ja) || (d == 3 && !is_pow2(p->ka))) {
+        int r = fail(h, BASTR_E_UNSUPPORTED, "grid %dx%dx%d: each extent must be a power of two in [16, 2048]",
+                     p->ia, p->ja, p->ka);
+        return r;
+    }
+    const int K = p->ia / 3;
+    if (p->ja < 2 * K || (d == 3 && p->ka < 2 * K)) {
+        int r = fail(h, BASTR_E_UNSUPPORTED, "ja and ka must be at least 2*floor(ia/3) (Nyquist modes dealiased)");
+        return r;
+    }
+    if (d == 3 && (p->ia > 512 || p->ja > 512 || p->ka > 512)) {
+        int r = fail(h, BASTR_E_UNSUPPORTED, "3D extents above 512 are not built");
+        return r;
+    }
+    h->fp32 = p->precision == BASTR_FP32;
+    Geo& g = h->g;
+    g.nx = p->ia; g.ny = p->ja; g.nz = nz; g.d = d; g.K = K;
+    g.KY = 2 * K - 1; g.KZ = d == 3 ? 2 * K - 1 : 1;
+    g.lproject = p->lprojectd ? 1 : 0;
+    g.nu = p->reynolds == 0.0 ? 0.0 : [&] {
+        const double tc = 110.4 / p->ref_tem, tc1 = 1.0 + tc;   // miucal(1.d0), solution.F90:1315-1329
+        return 1.0 * std::sqrt(1.0) * tc1 / (1.0 + tc);
+    }() / p->reynolds;
+    g.dt = p->deltat;
+    g.inv_n = 1.0 / ((double)p->ia * (double)p->ja * (double)nz);
+    h->allkmax = std::min(p->ia / 3, p->kmax);
+    if (h->allkmax < 0) h->allkmax = 0;
+    h->nshell = K + 1;
+    h->device = p->device;
+
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, BASTR_E_CUDA, "cudaSetDevice(%d) failed", h->device);
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+
+    const size_t cs = h->fp32 ? sizeof(float2) : sizeof(double2);
+    const size_t npts = (size_t)g.nx * g.ny * g.nz;
+    cudaError_t st = cudaSuccess;
+    if (d == 2) {
+        h->n_state = (size_t)K * g.KY * 2;
+        const size_t ma = std::max((size_t)g.ny * K * 7 * cs, (size_t)g.ny * K * 2 * sizeof(double2));
+        const size_t mb = (size_t)K * g.ny * 2 * std::max(cs, sizeof(double2));
+        dev_alloc(h, &h->ma, ma, st);
+        dev_alloc(h, &h->mb, mb, st);
+        h->n_vg_blocks = g.ny / (h->fp32 ? xpass_rows<float>(h, true) : xpass_rows<double>(h, true));
+        h->n_en_blocks = K;
+    } else {
+        h->n_state = (size_t)K * g.KY * g.KZ * 3;
+        size_t ma, mb, mc;
+        sizes3d(h, cs, ma, mb, mc);
+        dev_alloc(h, &h->ma, ma, st);
+        dev_alloc(h, &h->mb, mb, st);
+        dev_alloc(h, &h->mc, mc, st);
+        h->n_vg_blocks = vg_blocks3d(h);
+        h->n_en_blocks = en_blocks3d(h);
+    }
+    dev_alloc(h, &h->u0, h->n_state * sizeof(double2), st);
+    dev_alloc(h, &h->us, h->n_state * cs, st);
+    dev_alloc(h, &h->acc, h->n_state * cs, st);
+    dev_alloc(h, &h->phys, (size_t)d * npts * sizeof(double), st);
+    dev_alloc(h, &h->vg_part, (size_t)std::max(h->n_vg_blocks, 1) * 8 * sizeof(double), st);
+    dev_alloc(h, &h->en_part, (size_t)std::max(h->n_en_blocks, 1) * sizeof(double), st);
+    dev_alloc(h, &h->shell, (size_t)h->nshell * 4 * sizeof(double), st);
+    dev_alloc(h, &h->rec, (size_t)kChunk * R_COUNT * sizeof(double), st);
+    dev_alloc(h, &h->shells_dev, (size_t)kChunk * 2 * (h->allkmax + 1) * sizeof(double), st);
+    if (st != cudaSuccess) return fail(h, BASTR_E_CUDA, "device allocation failed: %s", cudaGetErrorString(st));
+
+    const int ns[3] = {g.nx, g.ny, d == 3 ? g.nz : 0};
+    for (int a = 0; a < 3; ++a) {
+        if (!ns[a]) continue;
+        std::vector<double2> t64;
+        std::vector<float2> t32;
+        host_twiddles(ns[a], t64, t32);
+        h->tw[a].n = ns[a];
+        CK(cudaMalloc(&h->tw[a].d64, ns[a] * sizeof(double2)));
+        CK(cudaMalloc(&h->tw[a].d32, ns[a] * sizeof(float2)));
+        CK(cudaMemcpy(h->tw[a].d64, t64.data(), ns[a] * sizeof(double2), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->tw[a].d32, t32.data(), ns[a] * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+    host_shells(h);
+    h->launches_per_step = count_launches(h, p->velgrad_every > 0);
+    CK(cudaDeviceSynchronize());
+    return BASTR_OK;
+}
+
+int bastr_destroy(bastr_handle* h) {
+    if (!h) return BASTR_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return BASTR_OK;
+}
+
+int bastr_set_state(bastr_handle* h, const double* u1, const double* u2, const double* u3) {
+    if (!h || !u1 || !u2 || (h->g.d == 3 && !u3)) return fail(h, BASTR_E_INVALID, "null field pointer");
+    CK(cudaSetDevice(h->device));
+    const size_t npts = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    const double* src[3] = {u1, u2, u3};
+    for (int c = 0; c < h->g.d; ++c)
+        CK(cudaMemcpyAsync(h->phys + c * npts, src[c], npts * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(to_spectral(h));
+    CK(cudaStreamSynchronize(h->stream));
+    h->have_state = true;
+    return BASTR_OK;
+}
+
+int bastr_get_state(bastr_handle* h, double* u1, double* u2, double* u3) {
+    if (!h || !u1 || !u2 || (h->g.d == 3 && !u3)) return fail(h, BASTR_E_INVALID, "null field pointer");
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    CK(cudaSetDevice(h->device));
+    CK(to_physical(h));
+    const size_t npts = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    double* dst[3] = {u1, u2, u3};
+    for (int c = 0; c < h->g.d; ++c)
+        CK(cudaMemcpyAsync(dst[c], h->phys + c * npts, npts * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return BASTR_OK;
+}
+
+int bastr_set_counters(bastr_handle* h, int64_t nstep, double time) {
+    if (!h) return BASTR_E_INVALID;
+    h->nstep = nstep;
+    h->time = time;
+    return BASTR_OK;
+}
+
+int bastr_get_counters(bastr_handle* h, int64_t* nstep, double* time) {
+    if (!h) return BASTR_E_INVALID;
+    if (nstep) *nstep = h->nstep;
+    if (time) *time = h->time;
+    return BASTR_OK;
+}
+
+int bastr_step_async(bastr_handle* h, int32_t nsteps) {
+    if (!h || nsteps < 0) return fail(h, BASTR_E_INVALID, "nsteps");
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    if (nsteps > kChunk) return fail(h, BASTR_E_INVALID, "bastr_step_async: at most %d steps per call", kChunk);
+    CK(cudaSetDevice(h->device));
+    h->batch_n0 = h->nstep;
+    h->batch_t0 = h->time;
+    for (int i = 0; i < nsteps; ++i) {
+        const int64_t n = h->nstep;
+        const bool vg = h->p.velgrad_every > 0 && (n % h->p.velgrad_every) == 0;
+        CK(launch_step(h, i, vg));
+        h->nstep += 1;
+        h->time = h->time + h->p.deltat;
+    }
+    h->chunk_used = nsteps;
+    return BASTR_OK;
+}
+
+int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells) {
+    if (!h) return BASTR_E_INVALID;
+    if (nsteps > h->chunk_used) return fail(h, BASTR_E_INVALID, "only %d records available", h->chunk_used);
+    CK(cudaSetDevice(h->device));
+    std::vector<double> rec((size_t)nsteps * R_COUNT);
+    if (nsteps) CK(cudaMemcpyAsync(rec.data(), h->rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (shells && nsteps)
+        CK(cudaMemcpyAsync(shells, h->shells_dev, (size_t)nsteps * 2 * (h->allkmax + 1) * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int64_t n0 = h->batch_n0;
+    double t = h->batch_t0;   // times accumulate exactly as the reference's time = time + deltat
+    for (int i = 0; i < nsteps; ++i) {
+        if (out) {
+            const double* r = &rec[(size_t)i * R_COUNT];
+            bastr_step_out& o = out[i];
+            o.nstep = n0 + i;
+            o.time = t;
+            o.Esspe = r[R_ES]; o.Edspe = r[R_ED]; o.k2Edspe = r[R_K2ED]; o.kMEdspe = r[R_KMED];
+            const bool vg = h->p.velgrad_every > 0 && ((n0 + i) % h->p.velgrad_every) == 0;
+            for (int k = 0; k < 8; ++k) o.velgrad[k] = vg ? r[R_VG0 + k] : NAN;
+            o.factor = h->p.forcemethod ? r[R_FACTOR] : NAN;
+            o.E = (h->p.forcemethod == 2 || h->p.forcemethod == 5) ? r[R_E] : NAN;
+        }
+        t = t + h->p.deltat;
+    }
+    return BASTR_OK;
+}
+
+int bastr_step(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells) {
+    if (!h || nsteps < 0) return fail(h, BASTR_E_INVALID, "nsteps");
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    int done = 0;
+    while (done < nsteps) {
+        const int n = std::min(kChunk, nsteps - done);
+        int r = bastr_step_async(h, n);
+        if (r) return r;
+        r = bastr_step_records(h, n, out ? out + done : nullptr,
+                               shells ? shells + (size_t)done * 2 * (h->allkmax + 1) : nullptr);
+        if (r) return r;
+        for (int i = 0; i < n && out; ++i) {
+            const bastr_step_out& o = out[done + i];
+            if (std::isnan(o.Esspe + o.Edspe)) {
+                return fail(h, BASTR_E_NAN, "\"E\" is a NaN at nstep %lld", (long long)o.nstep);
+            }
+        }
+        done += n;
+    }
+    return BASTR_OK;
+}
+
+int bastr_spectra(bastr_handle* h, double* kn, double* Es, double* Ed, int64_t* Ecount) {
+    if (!h) return BASTR_E_INVALID;
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    CK(cudaSetDevice(h->device));
+    const int am = h->allkmax;
+    // use the last chunk slot as scratch
+    double* rec = h->rec + (size_t)(kChunk - 1) * R_COUNT;
+    double* sh = h->shells_dev + (size_t)(kChunk - 1) * 2 * (am + 1);
+    CK(launch_spectra(h, rec, sh));
+    std::vector<double> buf(2 * (am + 1));
+    CK(cudaMemcpyAsync(buf.data(), sh, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int s = 0; s <= am; ++s) {
+        if (kn) kn[s] = h->kn[s];
+        if (Es) Es[s] = buf[s];
+        if (Ed) Ed[s] = buf[am + 1 + s];
+        if (Ecount) Ecount[s] = h->ecount[s];
+    }
+    return BASTR_OK;
+}
+
+int bastr_fft(bastr_handle* h, double* array, int32_t dir) {
+    if (!h || !array || (dir != 1 && dir != -1)) return fail(h, BASTR_E_INVALID, "bastr_fft arguments");
+    CK(cudaSetDevice(h->device));
+    return full_fft(h, array, dir);
+}
+
+int bastr_set_stream(bastr_handle* h, void* s) {
+    if (!h) return BASTR_E_INVALID;
+    CK(cudaSetDevice(h->device));
+    if (h->stream) CK(cudaStreamSynchronize(h->stream));
+    if (h->own_stream && h->stream) CK(cudaStreamDestroy(h->stream));
+    h->own_stream = false;
+    h->stream = (cudaStream_t)s;
+    return BASTR_OK;
+}
+
+int bastr_sync(bastr_handle* h) {
+    if (!h) return BASTR_E_INVALID;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    return BASTR_OK;
+}
+
+int bastr_info(bastr_handle* h, int32_t* allkmax, int32_t* launches, int64_t* bytes) {
+    if (!h) return BASTR_E_INVALID;
+    if (allkmax) *allkmax = h->allkmax;
+    if (launches) *launches = h->launches_per_step;
+    if (bytes) *bytes = h->dev_bytes;
+    return BASTR_OK;
+}
+
+int bastr_last_error(bastr_handle* h, char* buf, int32_t n) {
+    if (!h) return 0;
+    const int len = (int)h->err.size();
+    if (buf && n > 0) {
+        const int m = std::min(len, n - 1);
+        memcpy(buf, h->err.data(), m);
+        buf[m] = 0;
+    }
+    return len;
+}
+
+}  // extern "C"

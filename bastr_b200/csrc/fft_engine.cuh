@@ -1,0 +1,206 @@
+// Shared-memory Stockham FFT engine for sm_100a.
+//
+// A thread block transforms U independent complex sequences ("units") of length N that sit
+// in shared memory.  Each stage of radix R reads R elements per butterfly at stride N/R,
+// applies the twiddles, runs a register-resident DFT-R and writes the results in Stockham
+// autosort order, so the final stage leaves natural order without a bit-reversal pass.
+// Every thread holds all of its butterflies of one stage in registers between the read and
+// the write phase, which lets the stage run in place.
+//
+// Shared-memory addresses are padded by one element every 16 (pidx) so that the stride-R
+// writes of the first stages do not collide on the same banks.
+//
+// Twiddles come from a table tw[m] = exp(-2*pi*i*m/N) generated on the host in extended
+// precision and rounded once to the compute type; the inverse direction conjugates them.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bastr {
+
+template <typename T> struct cvec;
+template <> struct cvec<float>  { using t = float2; };
+template <> struct cvec<double> { using t = double2; };
+template <typename T> using cplx = typename cvec<T>::t;
+
+template <typename T> __device__ __forceinline__ cplx<T> mk(T x, T y) { cplx<T> r; r.x = x; r.y = y; return r; }
+template <typename T> __device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> __device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> __device__ __forceinline__ cplx<T> cscale(cplx<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
+template <typename T> __device__ __forceinline__ cplx<T> cconj(cplx<T> a) { return mk<T>(a.x, -a.y); }
+template <typename T> __device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
+    return mk<T>(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// multiply by i and by -i
+template <typename T> __device__ __forceinline__ cplx<T> cmuli(cplx<T> a) { return mk<T>(-a.y, a.x); }
+template <typename T> __device__ __forceinline__ cplx<T> cmulni(cplx<T> a) { return mk<T>(a.y, -a.x); }
+
+// Rotation by the quarter turn of the transform's sign: forward (sign -1) multiplies by -i,
+// inverse (sign +1) by +i.
+template <typename T, bool INV> __device__ __forceinline__ cplx<T> rot4(cplx<T> a) {
+    return INV ? cmuli<T>(a) : cmulni<T>(a);
+}
+
+// Padded shared-memory index: one spare slot every 16 elements.
+__device__ __forceinline__ int pidx(int a) { return a + (a >> 4); }
+__host__ __device__ constexpr int padded_len(int n) { return n + (n >> 4); }
+
+// ---------------------------------------------------------------------------------------
+// Register DFTs of size 2, 4, 8 and 16, natural order in and out.
+// ---------------------------------------------------------------------------------------
+template <typename T, bool INV> __device__ __forceinline__ void dft2(cplx<T>& a, cplx<T>& b) {
+    cplx<T> t = a;
+    a = cadd<T>(t, b);
+    b = csub<T>(t, b);
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft4(cplx<T>* v) {
+    cplx<T> s02 = cadd<T>(v[0], v[2]), d02 = csub<T>(v[0], v[2]);
+    cplx<T> s13 = cadd<T>(v[1], v[3]), d13 = rot4<T, INV>(csub<T>(v[1], v[3]));
+    v[0] = cadd<T>(s02, s13);
+    v[2] = csub<T>(s02, s13);
+    v[1] = cadd<T>(d02, d13);
+    v[3] = csub<T>(d02, d13);
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft8(cplx<T>* v) {
+    const T h = (T)0.70710678118654752440084436210484903928;  // sqrt(1/2)
+    cplx<T> e[4] = {v[0], v[2], v[4], v[6]};
+    cplx<T> o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<T, INV>(e);
+    dft4<T, INV>(o);
+    // o[k] *= exp(sign*i*pi*k/4)
+    const T sg = INV ? (T)1 : (T)-1;
+    o[1] = mk<T>(h * (o[1].x - sg * o[1].y), h * (o[1].y + sg * o[1].x));
+    o[2] = rot4<T, INV>(o[2]);
+    o[3] = mk<T>(-h * (o[3].x + sg * o[3].y), h * (sg * o[3].x - o[3].y));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        v[k] = cadd<T>(e[k], o[k]);
+        v[k + 4] = csub<T>(e[k], o[k]);
+    }
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft16(cplx<T>* v) {
+    // 16 = 4 x 4: columns n2, inner index n1 (x[4*n1 + n2])
+    const T c1 = (T)0.92387953251128675612818318939678828682;   // cos(pi/8)
+    const T s1 = (T)0.38268343236508977172845998403039886676;   // sin(pi/8)
+    const T h = (T)0.70710678118654752440084436210484903928;    // cos(pi/4)
+    const T sg = INV ? (T)1 : (T)-1;
+    cplx<T> y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+#pragma unroll
+        for (int n1 = 0; n1 < 4; ++n1) y[n2][n1] = v[4 * n1 + n2];
+        dft4<T, INV>(y[n2]);
+    }
+    // twiddle y[n2][k1] *= exp(sign*i*2*pi*n2*k1/16)
+    // n2 = 1: angles pi/8 * k1; n2 = 2: pi/4 * k1; n2 = 3: 3pi/8 * k1
+    const T cs[10] = {(T)1, c1, h, s1, (T)0, -s1, -h, -c1, (T)-1, -c1};
+    const T sn[10] = {(T)0, s1, h, c1, (T)1, c1, h, s1, (T)0, -s1};
+#pragma unroll
+    for (int n2 = 1; n2 < 4; ++n2) {
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1) {
+            const int m = n2 * k1;  // 1..9
+            cplx<T> w = mk<T>(cs[m], sg * sn[m]);
+            y[n2][k1] = cmul<T>(y[n2][k1], w);
+        }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        cplx<T> z[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+        dft4<T, INV>(z);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = z[k2];
+    }
+}
+
+template <typename T, bool INV, int R> __device__ __forceinline__ void dftR(cplx<T>* v) {
+    if constexpr (R == 2) dft2<T, INV>(v[0], v[1]);
+    else if constexpr (R == 4) dft4<T, INV>(v);
+    else if constexpr (R == 8) dft8<T, INV>(v);
+    else dft16<T, INV>(v);
+}
+
+// Radix of the next stage given the remaining factor REM = N / P.
+__host__ __device__ constexpr int next_radix(int rem) {
+    return (rem % 16 == 0 && rem != 32) ? 16 : (rem % 8 == 0) ? 8 : (rem % 4 == 0) ? 4 : 2;
+}
+
+// ---------------------------------------------------------------------------------------
+// One Stockham stage over U units.  Units come in groups of G: unit u starts at
+// s + (u/G)*GS + (u%G)*USTR (padded addressing inside a unit).
+// ---------------------------------------------------------------------------------------
+template <int G, int GS, int USTR> __device__ __forceinline__ int unit_off(int u) {
+    if constexpr (G == 1) return u * GS;
+    else return (u / G) * GS + (u % G) * USTR;
+}
+
+template <typename T, int N, int R, int P, int U, int USTR, int NT, bool INV, int G, int GS>
+__device__ __forceinline__ void fft_stage(cplx<T>* __restrict__ s, const cplx<T>* __restrict__ tw) {
+    constexpr int NB = N / R;          // butterflies per unit
+    constexpr int TOT = U * NB;
+    constexpr int PER = (TOT + NT - 1) / NT;
+    constexpr int TWS = N / (P * R);   // twiddle table stride
+    cplx<T> v[PER][R];
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int b = tid + q * NT;
+        if ((TOT % NT == 0) || b < TOT) {
+            const int u = b / NB, i = b - u * NB;
+            const int k = i & (P - 1);
+            cplx<T>* src = s + unit_off<G, GS, USTR>(u);
+#pragma unroll
+            for (int j = 0; j < R; ++j) v[q][j] = src[pidx(i + j * NB)];
+            if constexpr (P > 1) {
+#pragma unroll
+                for (int j = 1; j < R; ++j) {
+                    cplx<T> w = tw[j * k * TWS];
+                    if (INV) w.y = -w.y;
+                    v[q][j] = cmul<T>(v[q][j], w);
+                }
+            }
+            dftR<T, INV, R>(v[q]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int b = tid + q * NT;
+        if ((TOT % NT == 0) || b < TOT) {
+            const int u = b / NB, i = b - u * NB;
+            const int k = i & (P - 1);
+            cplx<T>* dst = s + unit_off<G, GS, USTR>(u);
+            const int base = (i - k) * R + k;
+#pragma unroll
+            for (int j = 0; j < R; ++j) dst[pidx(base + j * P)] = v[q][j];
+        }
+    }
+    __syncthreads();
+}
+
+// Full transform: all stages.  Unnormalised in both directions; forward uses exp(-i...).
+// The caller must __syncthreads() after filling the units.
+template <typename T, int N, int U, int USTR, int NT, bool INV, int G = U, int GS = U * USTR, int P = 1>
+__device__ __forceinline__ void fft_run(cplx<T>* __restrict__ s, const cplx<T>* __restrict__ tw) {
+    if constexpr (P < N) {
+        constexpr int R = next_radix(N / P);
+        fft_stage<T, N, R, P, U, USTR, NT, INV, G, GS>(s, tw);
+        fft_run<T, N, U, USTR, NT, INV, G, GS, P * R>(s, tw);
+    }
+}
+
+// Threads per block for U units of length N: each thread holds at most EPT complex values
+// per stage (16 doubles-complex = 64 registers, 32 floats-complex = 64 registers).
+template <typename T> __host__ __device__ constexpr int elems_per_thread() { return sizeof(T) == 8 ? 16 : 32; }
+template <typename T, int UN> __host__ __device__ constexpr int pick_threads() {
+    int nt = (UN + elems_per_thread<T>() - 1) / elems_per_thread<T>();
+    nt = ((nt + 31) / 32) * 32;
+    if (nt < 64) nt = 64;
+    if (nt > 1024) nt = 1024;
+    return nt;
+}
+
+}  // namespace bastr

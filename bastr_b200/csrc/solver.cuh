@@ -1,0 +1,196 @@
+// Geometry, layouts and launch helpers shared by the 2D/3D pass kernels.
+//
+// Spectral layout ("truncated half spectrum").  A real field has a Hermitian spectrum, so
+// only kx >= 0 is stored.  The spherical 2/3 rule of the reference (tool.F90:175-217) zeroes
+// every mode with |k| >= K = floor(ia/3); the state and every right-hand side therefore live
+// on kx in [0,K), ky and kz in (-K,K).  Those are the only modes kept in HBM:
+//
+//   S[kx][kyi][c]          2D, kyi in [0,KY), KY = 2K-1, c = velocity component
+//   S[kx][kyi][kzi][c]     3D, kzi in [0,KZ), KZ = 2K-1
+//
+// with index i < K meaning wavenumber i and i >= K meaning i - (2K-1) (negative side).
+// Modes outside this set are exactly zero in the reference's arithmetic up to round-off.
+#pragma once
+#include "fft_engine.cuh"
+
+namespace bastr {
+
+struct Geo {
+    int nx, ny, nz;     // grid (nz == 1 in 2D)
+    int d;              // 2 or 3
+    int K;              // dealias cutoff floor(nx/3); kept kx in [0,K)
+    int KY, KZ;         // truncated counts along y and z: 2K-1 (KZ == 1 in 2D)
+    int lproject;       // dilatational projection on the right-hand side
+    double nu, dt;
+    double inv_n;       // 1 / (nx*ny*nz)
+};
+
+// truncated index -> wavenumber, and -> position in a length-n transform
+__device__ __forceinline__ int trunc_k(int i, int K, int KT) { return i < K ? i : i - KT; }
+__device__ __forceinline__ int trunc_pos(int i, int K, int KT, int n) { return i < K ? i : i + (n - KT); }
+// position in a length-n transform -> truncated index, or -1 outside the kept set
+__device__ __forceinline__ int pos_trunc(int p, int K, int KT, int n) {
+    return p < K ? p : (p > n - K ? p - (n - KT) : -1);
+}
+
+template <typename A, typename B> __device__ __forceinline__ B cvt(A a);
+template <> __device__ __forceinline__ float2 cvt<double2, float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <> __device__ __forceinline__ double2 cvt<float2, double2>(float2 a) { return make_double2(a.x, a.y); }
+template <> __device__ __forceinline__ double2 cvt<double2, double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ float2 cvt<float2, float2>(float2 a) { return a; }
+
+__host__ __device__ constexpr int pow2_floor(int n) {
+    int p = 1;
+    while (p * 2 <= n) p *= 2;
+    return p;
+}
+
+// Fixed-order block reduction of NV doubles (sum) into every thread's v[]; the tree shape
+// depends only on the block size, so results are bitwise reproducible run to run.  Block
+// sizes that are not powers of two first fold their tail onto the leading power of two.
+template <int NV, int NT>
+__device__ __forceinline__ void block_sum(double* v, double* scratch /* NV*NT doubles */) {
+    constexpr int P2 = pow2_floor(NT);
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) scratch[i * NT + t] = v[i];
+    __syncthreads();
+    if constexpr (P2 != NT) {
+        if (t >= P2) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) scratch[i * NT + t - P2] += scratch[i * NT + t];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int s = P2 / 2; s > 0; s >>= 1) {
+        if (t < s) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) scratch[i * NT + t] += scratch[i * NT + t + s];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = scratch[i * NT];
+    __syncthreads();
+}
+
+template <int NT>
+__device__ __forceinline__ double block_min(double v, double* scratch) {
+    constexpr int P2 = pow2_floor(NT);
+    const int t = threadIdx.x;
+    scratch[t] = v;
+    __syncthreads();
+    if constexpr (P2 != NT) {
+        if (t >= P2) scratch[t - P2] = fmin(scratch[t - P2], scratch[t]);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int s = P2 / 2; s > 0; s >>= 1) {
+        if (t < s) scratch[t] = fmin(scratch[t], scratch[t + s]);
+        __syncthreads();
+    }
+    double r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+// Epilogue modes of the forward pass that closes a right-hand side evaluation.
+enum EpiMode : int {
+    EPI_STORE = 0,   // state <- dealiased spectrum (set_state)
+    EPI_RK1 = 1,     // k1; acc = k1; us = u0 + dt*k1/2
+    EPI_RK2 = 2,     // k2; us = u0 - dt*acc + 2dt*k2; acc += 4 k2
+    EPI_RK3 = 3,     // k3; u0 += dt*(acc + k3)/6
+    EPI_CN_MID = 4,  // Crank-Nicolson sweep 1..5: w = 0.5*((u0 + dt*k) + u0)
+    EPI_CN_LAST = 5, // sweep 6: u0 += dt*k
+};
+
+// Pointers a stage epilogue reads and writes (types per precision form).
+template <typename T>
+struct StageIO {
+    double2* u0;         // state, always FP64
+    cplx<T>* us;         // stage input of the next evaluation
+    cplx<T>* acc;        // RK accumulator k1 + 4 k2
+    double* energy_part; // per-block sum of w*|u0_new|^2 (RK3 / CN_LAST), or null
+};
+
+template <typename T>
+__device__ __forceinline__ double2 ld_stage(const StageIO<T>& io, size_t o, bool from_u0) {
+    return from_u0 ? io.u0[o] : cvt<cplx<T>, double2>(io.us[o]);
+}
+__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 dscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// Spectral epilogue of one mode (compute_ut, solution.F90:841-861 / 903-926, and the time
+// integrators, solution.F90:172-301).  v[c] holds the dealiased, 1/N-normalised transform of
+// the advective product; k[c] the wavenumbers, m2 = |k|^2; o the state offset of component 0;
+// w the Hermitian weight of the mode (1 on kx = 0, else 2); en accumulates w*|u0_new|^2.
+template <typename T, int D, int EPI>
+__device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double m2, size_t o,
+                                            const StageIO<T>& io, bool from_u0, const Geo& g,
+                                            double w, double& en) {
+    if constexpr (EPI == EPI_STORE) {
+#pragma unroll
+        for (int c = 0; c < D; ++c) io.u0[o + c] = v[c];
+        return;
+    } else {
+        const double nu = g.nu, dt = g.dt;
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            // + nu * FFT(lap u) with lap u^ = -|k|^2 u^
+            const double2 s = ld_stage<T>(io, o + c, from_u0);
+            v[c].x += nu * (-(s.x * m2));
+            v[c].y += nu * (-(s.y * m2));
+        }
+        if (g.lproject) {   // projection2D/3D, tool.F90:219-270
+            if (m2 > 0.25) {
+                const double kk = sqrt(m2);
+                double2 ud = make_double2(0, 0);
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    ud.x += v[c].x * k[c] / kk;
+                    ud.y += v[c].y * k[c] / kk;
+                }
+#pragma unroll
+                for (int c = 0; c < D; ++c) v[c] = make_double2(ud.x * k[c] / kk, ud.y * k[c] / kk);
+            } else {
+#pragma unroll
+                for (int c = 0; c < D; ++c) v[c] = make_double2(0, 0);
+            }
+        }
+        const double dt2 = 2.0 * dt;
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            const double2 a = io.u0[o + c];
+            if constexpr (EPI == EPI_RK1) {
+                io.acc[o + c] = cvt<double2, cplx<T>>(v[c]);
+                io.us[o + c] = cvt<double2, cplx<T>>(make_double2(a.x + dt * v[c].x / 2.0, a.y + dt * v[c].y / 2.0));
+            } else if constexpr (EPI == EPI_RK2) {
+                const double2 p = cvt<cplx<T>, double2>(io.acc[o + c]);
+                io.us[o + c] = cvt<double2, cplx<T>>(
+                    make_double2(a.x - dt * p.x + dt2 * v[c].x, a.y - dt * p.y + dt2 * v[c].y));
+                io.acc[o + c] = cvt<double2, cplx<T>>(make_double2(p.x + 4.0 * v[c].x, p.y + 4.0 * v[c].y));
+            } else if constexpr (EPI == EPI_RK3) {
+                const double2 p = cvt<cplx<T>, double2>(io.acc[o + c]);
+                const double2 n = make_double2(a.x + dt * (p.x + v[c].x) / 6.0, a.y + dt * (p.y + v[c].y) / 6.0);
+                io.u0[o + c] = n;
+                en += w * (n.x * n.x + n.y * n.y);
+            } else if constexpr (EPI == EPI_CN_MID) {
+                io.us[o + c] = cvt<double2, cplx<T>>(
+                    make_double2(0.5 * ((a.x + dt * v[c].x) + a.x), 0.5 * ((a.y + dt * v[c].y) + a.y)));
+            } else if constexpr (EPI == EPI_CN_LAST) {
+                const double2 n = make_double2(a.x + dt * v[c].x, a.y + dt * v[c].y);
+                io.u0[o + c] = n;
+                en += w * (n.x * n.x + n.y * n.y);
+            }
+        }
+    }
+}
+
+// Lines (or rows) per block so that one block holds about 48 KB of transform data; a power of 2.
+template <typename T> __host__ __device__ constexpr int target_elems() { return sizeof(T) == 8 ? 3072 : 6144; }
+template <typename T, int N, int F> __host__ __device__ constexpr int lines_per_block() {
+    return pow2_floor(target_elems<T>() / (F * N));
+}
+
+}  // namespace bastr

@@ -1,0 +1,126 @@
+/*
+ * bastr_gpu.h -- C ABI of the B200 (sm_100a) pseudo-spectral Burgers time step.
+ *
+ * The library replaces the FFTW-MPI hot path of Bastr (lcs27/Bastr).  A Fortran driver
+ * binds these entry points with iso_c_binding; every function returns an int status
+ * (0 = ok, < 0 = error, message via bastr_last_error), plain pointers and sizes only.
+ *
+ * Entry point                 replaces (reference file:line)
+ * --------------------------  ---------------------------------------------------------------
+ * bastr_create                readinput derivations (readwrite.F90:69-83), mpisizedis_fftw
+ *                             (fftwlink.F90:34-153), allocation (fftwlink.F90:370-467),
+ *                             prepareplan_fftw_plan (fftwlink.F90:284-303), quantity_prepare
+ *                             (solution.F90:1288-1313)
+ * bastr_set_state             the initial dealias of mainloop2D/3D (solution.F90:41-52,
+ *                             106-122) applied to u1,u2[,u3] after read_initial_field /
+ *                             read_continue_field (readwrite.F90:114-220)
+ * bastr_set_counters          nstep/time restored by read_continue_field (readwrite.F90:211-218)
+ * bastr_step                  n iterations of the `do while(nstep<=maxstep)` body of
+ *                             mainloop2D/3D (solution.F90:54-97, 124-169): spectra_compute,
+ *                             velgrad_calculate, nstep/time advance, RK3 or CN, forcing
+ * bastr_get_state             the physical u1,u2[,u3] that writeflfed dumps (readwrite.F90:222-257)
+ * bastr_spectra               spectra_compute2D/3D shell arrays (solution.F90:930-1108)
+ * bastr_fft                   fft2d/fft3d/ifft2d/ifft3d (fftwlink.F90:324-368), in place on a
+ *                             full complex(8) grid, for Bastrpp-style callers
+ * bastr_destroy               deallocation (fftwlink.F90:469-490)
+ * bastr_last_error            the reference's `stop 'message'` text, as a return value
+ *
+ * Layout: fields are real(8) arrays in Fortran order u(1:ia,1:ja[,1:ka]), x fastest,
+ * which is C order [ka][ja][ia].
+ *
+ * A handle owns one stream on one GPU and is not thread-safe; use one handle per GPU.
+ */
+#ifndef BASTR_GPU_H
+#define BASTR_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BASTR_API __attribute__((visibility("default")))
+#else
+#define BASTR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BASTR_OK 0
+#define BASTR_E_INVALID (-1)     /* bad argument or parameter */
+#define BASTR_E_UNSUPPORTED (-2) /* valid for the reference, not built here (e.g. grid size) */
+#define BASTR_E_CUDA (-3)        /* CUDA runtime error */
+#define BASTR_E_NAN (-4)         /* Es+Ed became NaN (solution.F90:81): stepping stopped */
+#define BASTR_E_STATE (-5)       /* call order: no state set yet */
+
+#define BASTR_FP64 0             /* FP64 fields and transforms: parity form */
+#define BASTR_FP32 1             /* FP32 fields/transforms/product, FP64 state and reductions */
+
+/* The datin/input.dat values the time step reads (readwrite.F90:35-44), plus GPU knobs. */
+typedef struct bastr_params {
+    int32_t ia, ja, ka;          /* grid; ka == 0 selects 2D */
+    double ref_tem, reynolds;    /* nu = miucal(1)/reynolds = 1/reynolds; reynolds == 0 -> nu = 0 */
+    double deltat;
+    int32_t kmax;                /* allkmax = min(ia/3, kmax) */
+    int32_t timemethod;          /* 1 = RK3 (Kutta), 2 = Crank-Nicolson 6-sweep fixed point */
+    int32_t forcemethod;         /* 0 none, 1 linear, 2 band, 5 band to target (3/4: unsupported) */
+    int32_t forcek;
+    double target_energy;
+    int32_t lprojectd;           /* project the right-hand side on its dilatational part */
+    int32_t precision;           /* BASTR_FP64 or BASTR_FP32 */
+    int32_t device;              /* CUDA device ordinal */
+    int32_t velgrad_every;       /* velocity-gradient statistics every n steps (1 = reference; 0 = never) */
+} bastr_params;
+
+/* One iteration of the main loop.  nstep/time are the values the reference logs with the
+ * spectra and velgrad lines (before the increment); the forcing line uses nstep+1, time+dt. */
+typedef struct bastr_step_out {
+    int64_t nstep;
+    double time;
+    double Esspe, Edspe, k2Edspe, kMEdspe;      /* log/stat{2,3}d_specall.dat */
+    double velgrad[8];                          /* umumtheta2 umumijji u2theta dissp etamin Tay ReTay Kol */
+    double factor, E;                           /* log/factor_output.dat (NaN when not written) */
+} bastr_step_out;
+
+typedef struct bastr_handle bastr_handle;
+
+BASTR_API int bastr_create(const bastr_params* p, bastr_handle** out);
+BASTR_API int bastr_destroy(bastr_handle* h);
+
+/* Host arrays, x fastest; u3 ignored in 2D. */
+BASTR_API int bastr_set_state(bastr_handle* h, const double* u1, const double* u2, const double* u3);
+BASTR_API int bastr_get_state(bastr_handle* h, double* u1, double* u2, double* u3);
+BASTR_API int bastr_set_counters(bastr_handle* h, int64_t nstep, double time);
+BASTR_API int bastr_get_counters(bastr_handle* h, int64_t* nstep, double* time);
+
+/* Runs nsteps iterations; out[nsteps] (may be NULL); shells (may be NULL) receives, per step,
+ * Es[0..allkmax] then Ed[0..allkmax].  Returns BASTR_E_NAN at the first step whose Es+Ed is NaN
+ * (that step's record is filled; the state is the one that produced the NaN). */
+BASTR_API int bastr_step(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells);
+
+/* Enqueues nsteps iterations on the handle's stream and returns without synchronising;
+ * per-step records stay on the device (bastr_step_records copies the last batch). */
+BASTR_API int bastr_step_async(bastr_handle* h, int32_t nsteps);
+BASTR_API int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells);
+
+/* Shell spectra of the current state: arrays of allkmax+1 entries (shell 0..allkmax). */
+BASTR_API int bastr_spectra(bastr_handle* h, double* kn, double* Es, double* Ed, int64_t* Ecount);
+
+/* In-place c2c transform of a full complex(8) grid (interleaved re,im; x fastest):
+ * dir = -1 forward scaled by 1/N (fft2d/fft3d), dir = +1 backward unscaled (ifft2d/ifft3d). */
+BASTR_API int bastr_fft(bastr_handle* h, double* array, int32_t dir);
+
+/* Stream control for callers that time or order work around the library. */
+BASTR_API int bastr_set_stream(bastr_handle* h, void* cuda_stream);
+BASTR_API int bastr_sync(bastr_handle* h);
+
+/* Introspection: allkmax, kernels launched per step, device bytes held. */
+BASTR_API int bastr_info(bastr_handle* h, int32_t* allkmax, int32_t* launches_per_step, int64_t* device_bytes);
+
+/* Copies the message of the last failed call into buf (NUL-terminated); returns its length. */
+BASTR_API int bastr_last_error(bastr_handle* h, char* buf, int32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BASTR_GPU_H */

@@ -1,0 +1,453 @@
+"""CPU oracle for the Bastr pseudo-spectral Burgers time step (test infrastructure only).
+
+This module is the checker, not the product.  Only ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline legs of ``bench.py`` may import it.  The product path (the CUDA
+library under ``bastr_b200/csrc``) never calls into it.
+
+It is a line-by-line FP64 restatement of the reference's Fortran hot path, with the same
+complex-to-complex transforms, normalisation and quirks:
+
+* ``fft``/``ifft``           -- fftwlink.F90:324-368 (forward e^{-ikx} scaled by 1/N, backward raw)
+* ``generate_wave``          -- tool.F90:17-96
+* ``kint``                   -- tool.F90:126-147 (method 2: nint(k/dk))
+* ``dealiasing``             -- tool.F90:149-217 (zero where |k| >= floor(ia/3), all axes use ia)
+* ``projection``             -- tool.F90:219-270
+* ``compute_ut``             -- solution.F90:816-928
+* ``rk3`` / ``cn``           -- solution.F90:172-301
+* ``forcing``                -- solution.F90:303-814 (methods 0, 1, 2, 5; 3/4 use gfortran's RNG)
+* ``spectra_compute``        -- solution.F90:930-1108
+* ``velgrad_calculate``      -- solution.F90:1110-1286
+* ``quantity_prepare``/``miucal`` -- solution.F90:1288-1329
+* ``readinput`` derivations  -- readwrite.F90:69-83 (ndims, allkmax)
+* ``mainloop``               -- solution.F90:20-170
+* ``listwrite`` format       -- utility.F90:87-164 ``(1X,I20,n(1X,E20.13E2))``
+
+Layout: fields are NumPy arrays in C order ``(ny, nx)`` for 2D and ``(nz, ny, nx)`` for 3D,
+i.e. the same bytes as the reference's Fortran ``u(1:im,1:jm[,1:km])`` with x fastest.
+
+Parity status: unpinned.  The reference ships no tests, fixtures or golden outputs, and it
+cannot be built here (no Fortran compiler, MPI, FFTW or HDF5).  The restatement is pinned only
+by analytic known-answer tests (single-mode transforms and derivatives, Parseval, linear
+viscous decay, the 1-D Burgers Cole-Hopf solution embedded in 2D/3D) in ``tests/``.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+try:  # scipy's pocketfft runs multi-threaded; numpy's is the fallback
+    import scipy.fft as _sfft
+
+    def _fftn(a, workers):
+        return _sfft.fftn(a, workers=workers)
+
+    def _ifftn(a, workers):
+        return _sfft.ifftn(a, workers=workers)
+except ImportError:  # pragma: no cover
+    def _fftn(a, workers):
+        return np.fft.fftn(a)
+
+    def _ifftn(a, workers):
+        return np.fft.ifftn(a)
+
+
+# ---------------------------------------------------------------------------------------
+# parameters (commvar.F90:16-66, readwrite.F90:19-112, solution.F90:1288-1329)
+# ---------------------------------------------------------------------------------------
+@dataclass
+class Params:
+    """The ``datin/input.dat`` values the hot path reads (readwrite.F90:35-44)."""
+    ia: int
+    ja: int
+    ka: int = 0
+    ref_tem: float = 273.15
+    reynolds: float = 5000.0
+    maxstep: int = 10
+    deltat: float = 1e-4
+    lwsequ: bool = False
+    feqwsequ: int = 1000000
+    lwspectra: bool = True
+    feqwspe: int = 50
+    kmax: int = 1 << 30
+    timemethod: int = 1
+    forcemethod: int = 0
+    forcek: int = 5
+    target_energy: float = 0.075
+    lprojectd: bool = False
+
+    @property
+    def ndims(self) -> int:
+        """readwrite.F90:69-80."""
+        if self.ka == 0:
+            if self.ja == 0:
+                raise ValueError("1D case is not implemented yet!")
+            return 2
+        return 3
+
+    @property
+    def allkmax(self) -> int:
+        """readwrite.F90:75-83: min(int(ia/3), kmax)."""
+        return min(self.ia // 3, self.kmax)
+
+    @property
+    def nu(self) -> float:
+        """solution.F90:1306-1310 with miucal (solution.F90:1315-1329) at T=1."""
+        if self.reynolds == 0.0:
+            return 0.0
+        return miucal(1.0, self.ref_tem) / self.reynolds
+
+    @property
+    def shape(self):
+        return (self.ja, self.ia) if self.ndims == 2 else (self.ka, self.ja, self.ia)
+
+    @property
+    def npts(self) -> int:
+        return int(np.prod(self.shape))
+
+
+def miucal(temper: float, ref_tem: float) -> float:
+    """Sutherland law, solution.F90:1315-1329 (equals 1 at temper=1)."""
+    tempconst = 110.4 / ref_tem
+    tempconst1 = 1.0 + tempconst
+    return temper * math.sqrt(temper) * tempconst1 / (temper + tempconst)
+
+
+# ---------------------------------------------------------------------------------------
+# spectral tools (tool.F90)
+# ---------------------------------------------------------------------------------------
+def wavenumbers_1d(n: int) -> np.ndarray:
+    """tool.F90:31-37: index i (1-based) <= n/2+1 -> i-1, else i-n-1 (Nyquist is +n/2)."""
+    i = np.arange(n)
+    return np.where(i <= n // 2, i, i - n).astype(np.float64)
+
+
+def generate_wave(p: Params):
+    """tool.F90:17-96.  Returns k1, k2[, k3] broadcast to the field shape."""
+    kx = wavenumbers_1d(p.ia)
+    ky = wavenumbers_1d(p.ja)
+    if p.ndims == 2:
+        k1 = np.broadcast_to(kx[None, :], p.shape).copy()
+        k2 = np.broadcast_to(ky[:, None], p.shape).copy()
+        return k1, k2
+    kz = wavenumbers_1d(p.ka)
+    k1 = np.broadcast_to(kx[None, None, :], p.shape).copy()
+    k2 = np.broadcast_to(ky[None, :, None], p.shape).copy()
+    k3 = np.broadcast_to(kz[:, None, None], p.shape).copy()
+    return k1, k2, k3
+
+
+def kint(k, dk=1.0):
+    """tool.F90:126-147, method 2: Fortran NINT (half away from zero; k >= 0 here)."""
+    return np.floor(np.asarray(k) / dk + 0.5).astype(np.int64)
+
+
+def dealias_mask(p: Params, kk: np.ndarray, factor: int = 3) -> np.ndarray:
+    """tool.F90:185-193 / 206-214: True where the mode is KEPT (|k| < floor(ia/factor))."""
+    cutoff = math.floor(float(p.ia) / float(factor))
+    return ~(kk >= cutoff)
+
+
+# ---------------------------------------------------------------------------------------
+# the solver state, a restatement of the reference's module globals
+# ---------------------------------------------------------------------------------------
+@dataclass
+class StepRecord:
+    nstep: int
+    time: float
+    Esspe: float
+    Edspe: float
+    k2Edspe: float
+    kMEdspe: float
+    velgrad: tuple            # umumtheta2, umumijji, u2theta, dissp, eta_min, Tay, ReTay, Kol
+    forcing: tuple | None     # (factor[, E]) written after the RK step, or None
+    spect: tuple | None       # (kn, Es, Ed) shells 1..allkmax when written, else None
+
+
+class Oracle:
+    """Restatement of mainloop2D/3D and everything it calls, in FP64 with c2c transforms."""
+
+    def __init__(self, p: Params, u, workers: int | None = None):
+        if p.timemethod not in (1, 2):
+            raise ValueError("Undefined time method")  # readwrite.F90:98-104
+        if p.forcemethod in (3, 4):
+            raise NotImplementedError("forcing methods 3/4 draw from gfortran's random_number")
+        self.p = p
+        self.workers = workers if workers is not None else (os.cpu_count() or 1)
+        self.ks = generate_wave(p)
+        self.kk2 = sum(k * k for k in self.ks)
+        self.kk = np.sqrt(self.kk2)
+        self.nu = p.nu
+        self.u = [np.array(c, dtype=np.float64, copy=True).reshape(p.shape) for c in u]
+        if len(self.u) != p.ndims:
+            raise ValueError("need one velocity component per dimension")
+        # quantity_prepare (solution.F90:1288-1313)
+        self.nstep = 0
+        self.time = 0.0
+        self.nxtwsequ = min(p.feqwsequ, p.maxstep)
+        self.nxtwspe = 0
+        self.filenumb = 1
+        self.N = float(p.npts)
+        self._mask = dealias_mask(p, self.kk)
+        self.dumps = []
+
+    # -- fftwlink.F90:324-368 ------------------------------------------------------------
+    def fft(self, a):
+        return _fftn(np.asarray(a, dtype=np.complex128), self.workers) / (1.0 * self.N)
+
+    def ifft(self, a):
+        return _ifftn(np.asarray(a, dtype=np.complex128), self.workers) * self.N
+
+    # -- tool.F90 -------------------------------------------------------------------------
+    def dealiasing(self, f):
+        return np.where(self._mask, f, 0.0)
+
+    def projection(self, fs):
+        kk = self.kk
+        big = kk > 0.5
+        safe = np.where(big, kk, 1.0)
+        ud = sum(f * k / safe for f, k in zip(fs, self.ks))
+        return [np.where(big, ud * k / safe, 0.0) for k in self.ks]
+
+    # -- solution.F90:816-928 -------------------------------------------------------------
+    def compute_ut(self, uspe):
+        """Returns (u_t list, physical uspe list); both complex like the reference."""
+        p, ks, nu = self.p, self.ks, self.nu
+        I = 1j
+        d = p.ndims
+        grads = [[self.ifft(I * uspe[i] * ks[j]) for j in range(d)] for i in range(d)]
+        lap = [self.ifft(-uspe[i] * self.kk2) for i in range(d)]
+        uphys = [self.ifft(uspe[i]) for i in range(d)]
+        if d == 2:
+            # solution.F90:841-846 uses dreal() of every factor
+            ut = []
+            for i in range(2):
+                t = (-uphys[0].real * grads[i][0].real
+                     - uphys[1].real * grads[i][1].real
+                     + nu * lap[i].real)
+                ut.append(t.astype(np.complex128))
+        else:
+            # solution.F90:903-908 multiplies the COMPLEX physical u by dreal(derivatives)
+            ut = []
+            for i in range(3):
+                t = (-uphys[0] * grads[i][0].real - uphys[1] * grads[i][1].real
+                     - uphys[2] * grads[i][2].real + nu * lap[i].real)
+                ut.append(t)
+        ut = [self.dealiasing(self.fft(t)) for t in ut]
+        if p.lprojectd:
+            ut = self.projection(ut)
+        ut = [self.ifft(t) for t in ut]
+        return ut, uphys
+
+    # -- solution.F90:172-203, 233-270 ----------------------------------------------------
+    def rk3(self):
+        dt = self.p.deltat
+        uspe = [self.fft(c) for c in self.u]
+        kA, _ = self.compute_ut(uspe)
+        uspe = [self.fft((c + dt * a.real / 2.0).astype(np.complex128)) for c, a in zip(self.u, kA)]
+        kB, _ = self.compute_ut(uspe)
+        uspe = [self.fft((c - dt * a.real + 2.0 * dt * b.real).astype(np.complex128))
+                for c, a, b in zip(self.u, kA, kB)]
+        kC, _ = self.compute_ut(uspe)
+        self.u = [c + dt * (a.real + 4.0 * b.real + cc.real) / 6.0
+                  for c, a, b, cc in zip(self.u, kA, kB, kC)]
+
+    # -- solution.F90:205-231, 272-301 ----------------------------------------------------
+    def cn(self):
+        dt = self.p.deltat
+        uold = [c.copy() for c in self.u]
+        uspe = [self.fft(c) for c in self.u]
+        for step in range(1, 7):
+            kA, _ = self.compute_ut(uspe)
+            self.u = [o + dt * a.real for o, a in zip(uold, kA)]
+            if step == 6:
+                break
+            uspe = [self.fft(0.5 * (c + o)) for c, o in zip(self.u, uold)]
+
+    # -- solution.F90:303-814 -------------------------------------------------------------
+    def forcing(self):
+        p = self.p
+        m = p.forcemethod
+        N = self.N
+        if m == 0:
+            return None
+        if m == 1:
+            energy = float(np.sum(sum(c ** 2 for c in self.u) / 2.0)) / N
+            factor = math.sqrt(p.target_energy / energy)
+            self.u = [factor * c for c in self.u]
+            return (factor,)
+        if m in (2, 5):
+            dk = 0.5
+            uspe = [self.fft(c) for c in self.u]
+            kk = self.kk
+            band = ((kk - dk) < p.forcek) & ((kk + dk) > p.forcek)
+            if m == 5 and p.ndims == 2 and p.lprojectd:
+                safe = np.where(band, kk, 1.0)
+                ud = uspe[0] * self.ks[0] / safe + uspe[1] * self.ks[1] / safe
+                force = [np.where(band, ud * k / safe, 0.0) for k in self.ks]
+            else:
+                force = [np.where(band, s, 0.0) for s in uspe]
+            # the 3D method-5 path calls ifft2d on force1/2; both wrap backward_plan (fftwlink.F90:350-368)
+            force = [self.ifft(f) for f in force]
+            E = float(np.sum(sum(f.real ** 2 for f in force))) / N
+            if m == 2:
+                factor = math.sqrt(p.target_energy / E) - 1.0
+            else:
+                energy = float(np.sum(sum(c ** 2 for c in self.u))) / N
+                if p.target_energy > energy:
+                    factor = math.sqrt((p.target_energy - energy) / E + 1.0) - 1.0
+                else:
+                    factor = 0.0
+            self.u = [c + factor * f.real for c, f in zip(self.u, force)]
+            return (factor, E)
+        raise NotImplementedError(f"forcemethod {m}")
+
+    # -- solution.F90:930-1108 ------------------------------------------------------------
+    def spectra_compute(self, uspe):
+        p = self.p
+        kk = self.kk
+        big = kk > 0.5
+        safe = np.where(big, kk, 1.0)
+        if p.ndims == 2:
+            k1, k2 = self.ks
+            us = np.where(big, uspe[0] * k2 / safe - uspe[1] * k1 / safe, 0.0)
+            ud = np.where(big, uspe[0] * k1 / safe + uspe[1] * k2 / safe, 0.0)
+            es_mode = (us * np.conj(us)).real / 2
+        else:
+            ud = np.where(big, sum(s * k / safe for s, k in zip(uspe, self.ks)), 0.0)
+            es_mode = 0.0
+            for s, k in zip(uspe, self.ks):
+                usi = np.where(big, s - ud * k / safe, 0.0)
+                es_mode = es_mode + (usi * np.conj(usi)).real / 2
+        ed_mode = (ud * np.conj(ud)).real / 2
+        kMEd = float(np.sum(np.where(big, ed_mode / safe, 0.0)))
+        sh = kint(kk, 1.0).ravel()
+        am = p.allkmax
+        sel = sh <= am
+        Ecount = np.bincount(sh[sel], minlength=am + 1)[: am + 1].astype(np.int64)
+        Es = np.bincount(sh[sel], weights=np.ravel(es_mode)[sel], minlength=am + 1)[: am + 1]
+        Ed = np.bincount(sh[sel], weights=np.ravel(ed_mode)[sel], minlength=am + 1)[: am + 1]
+        kn = np.bincount(sh[sel], weights=kk.ravel()[sel], minlength=am + 1)[: am + 1]
+        kn = kn.copy()
+        for i in range(1, am + 1):  # solution.F90:991-996: shells 1..allkmax are normalised
+            kn[i] = kn[i] / Ecount[i] if Ecount[i] else float("nan")
+        return dict(Es=Es, Ed=Ed, kn=kn, Ecount=Ecount,
+                    Edspe=float(np.sum(ed_mode)), Esspe=float(np.sum(es_mode)),
+                    k2Edspe=float(np.sum(ed_mode * kk * kk)), kMEdspe=kMEd)
+
+    # -- solution.F90:1110-1286 -----------------------------------------------------------
+    def velgrad_calculate(self, uspe):
+        p, nu = self.p, self.nu
+        d = p.ndims
+        I = 1j
+        ks = self.ks
+        kk2 = self.kk2
+        g = [[self.ifft(I * uspe[i] * ks[j]).real for j in range(d)] for i in range(d)]
+        lap = [self.ifft(-uspe[i] * kk2).real for i in range(d)]
+        th = self.ifft(-I * sum(uspe[i] * ks[i] * kk2 for i in range(d))).real
+        u = self.u
+        N = self.N
+        div = sum(g[i][i] for i in range(d))
+        uu = sum(c ** 2 for c in u)
+        umumtheta2 = float(np.sum(div ** 2 * uu)) / N
+        ijji = sum(g[i][i] ** 2 for i in range(d))
+        for i in range(d):
+            for j in range(i + 1, d):
+                ijji = ijji + 2.0 * g[i][j] * g[j][i]
+        umumijji = float(np.sum(ijji * uu)) / N
+        u2theta = float(np.sum(div * uu)) / N
+        dissp = sum(2.0 * u[i] * div * lap[i] for i in range(d)) + uu * th
+        dissp = float(np.sum(dissp)) / N
+        eps = nu * div ** 2
+        for (i, j) in ([(0, 1)] if d == 2 else [(0, 1), (1, 2), (0, 2)]):
+            eps = eps + nu * (g[i][j] - g[j][i]) ** 2
+        epsilon = float(np.sum(eps)) / N
+        # eta_min starts at the default-real literal 2*3.14 (solution.F90:1145, 1236)
+        eta0 = float(np.float32(2) * np.float32(3.14))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            eta_pts = np.sqrt(nu / np.abs(div))
+        eta_min = min(eta0, float(np.nanmin(eta_pts))) if eta_pts.size else eta0
+        urms = math.sqrt(float(np.sum(uu)) / N)
+        dudx2 = float(np.sum(sum(g[i][i] ** 2 for i in range(d)))) / N
+        ufluc = urms / math.sqrt(float(d))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            tay = ufluc / math.sqrt(dudx2 / float(d)) if dudx2 > 0 else float("inf")
+            retay = ufluc * tay / nu if nu != 0 else float("inf")
+            kol = math.sqrt(math.sqrt(nu ** 3 / epsilon)) if epsilon > 0 else float("inf")
+        return (umumtheta2, umumijji, u2theta, dissp, eta_min, tay, retay, kol)
+
+    # -- solution.F90:36-170 --------------------------------------------------------------
+    def initial_dealias(self):
+        """solution.F90:41-52 / 106-122."""
+        self.u = [self.ifft(self.dealiasing(self.fft(c))).real for c in self.u]
+
+    def step_once(self, do_velgrad: bool = True) -> StepRecord:
+        """One iteration of the `do while(nstep<=maxstep)` body."""
+        p = self.p
+        uspe = [self.fft(c) for c in self.u]
+        sp = self.spectra_compute(uspe)
+        spect = None
+        if p.lwspectra and self.nstep == self.nxtwspe:
+            spect = (sp["kn"][1:].copy(), sp["Es"][1:].copy(), sp["Ed"][1:].copy())
+            self.nxtwspe = min(self.nxtwspe + p.feqwspe, p.maxstep)
+        vg = self.velgrad_calculate(uspe) if do_velgrad else None
+        rec_n, rec_t = self.nstep, self.time
+        E = sp["Esspe"] + sp["Edspe"]
+        if (p.lwsequ and self.nstep == self.nxtwsequ) or math.isnan(E):
+            self.dumps.append((self.filenumb, self.nstep, self.time, [c.copy() for c in self.u]))
+            self.filenumb += 1
+            self.nxtwsequ = min(self.nxtwsequ + p.feqwsequ, p.maxstep)
+        if math.isnan(E):
+            raise FloatingPointError('"E" is a NaN')
+        self.nstep += 1
+        self.time += p.deltat
+        if p.timemethod == 1:
+            self.rk3()
+        else:
+            self.cn()
+        fo = self.forcing()
+        return StepRecord(rec_n, rec_t, sp["Esspe"], sp["Edspe"], sp["k2Edspe"], sp["kMEdspe"],
+                          vg, fo, spect), sp
+
+    def mainloop(self, nsteps: int | None = None, do_velgrad: bool = True):
+        """Runs the loop; ``nsteps`` bounds the number of iterations (default: maxstep+1)."""
+        self.initial_dealias()
+        recs = []
+        n = 0
+        while self.nstep <= self.p.maxstep and (nsteps is None or n < nsteps):
+            rec, _ = self.step_once(do_velgrad)
+            recs.append(rec)
+            n += 1
+        return recs
+
+
+# ---------------------------------------------------------------------------------------
+# log format (utility.F90:87-164)
+# ---------------------------------------------------------------------------------------
+def fortran_e20_13(x: float) -> str:
+    """Fortran ``E20.13E2``: ' 0.ddddddddddddd E+ee' right-justified in 20 columns."""
+    if x != x:
+        return "NaN".rjust(20)
+    if math.isinf(x):
+        return ("-Infinity" if x < 0 else "Infinity").rjust(20)
+    if x == 0.0:
+        s = "0.0000000000000E+00"
+        return (("-" + s) if math.copysign(1.0, x) < 0 else s).rjust(20)
+    m, e = f"{abs(x):.12e}".split("e")  # d.dddddddddddd (13 significant digits)
+    e = int(e) + 1
+    digits = m.replace(".", "")
+    if abs(e) <= 99:
+        es = f"E{'+' if e >= 0 else '-'}{abs(e):02d}"
+    else:
+        es = f"{'+' if e >= 0 else '-'}{abs(e):03d}"
+    s = f"0.{digits}{es}"
+    if x < 0:
+        s = "-" + s
+    return s.rjust(20)
+
+
+def listwrite_line(nstep: int, time: float, *vals: float) -> str:
+    """utility.F90:87-164: ``(1X,I20,n(1X,E20.13E2))`` with time/ref_tim (ref_tim = 1)."""
+    return " " + f"{nstep:20d}" + "".join(" " + fortran_e20_13(v) for v in (time, *vals))
