@@ -37,7 +37,7 @@ BASTR_FP32 = 1
 EXPORTED = [
     "bastr_create", "bastr_destroy", "bastr_set_state", "bastr_get_state", "bastr_set_counters",
     "bastr_get_counters", "bastr_step", "bastr_step_async", "bastr_step_records", "bastr_spectra",
-    "bastr_fft", "bastr_set_stream", "bastr_sync", "bastr_info", "bastr_last_error",
+    "bastr_fft", "bastr_set_stream", "bastr_sync", "bastr_info", "bastr_last_error", "bastr_profile",
 ]
 
 
@@ -63,6 +63,11 @@ class CStepOut(C.Structure):
         ("Esspe", C.c_double), ("Edspe", C.c_double), ("k2Edspe", C.c_double), ("kMEdspe", C.c_double),
         ("velgrad", C.c_double * 8), ("factor", C.c_double), ("E", C.c_double),
     ]
+
+
+class CKernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("launches", C.c_int32), ("total_ms", C.c_double),
+                ("bytes_per_launch", C.c_double)]
 
 
 _lib = None
@@ -93,6 +98,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_sync.argtypes = [P]
     lib.bastr_info.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     lib.bastr_last_error.argtypes = [P, C.c_char_p, C.c_int32]
+    lib.bastr_profile.argtypes = [P, C.c_int32, C.POINTER(CKernelStat), C.c_int32, C.POINTER(C.c_int32)]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -241,6 +247,15 @@ class BastrGPU:
         self._check(self.lib.bastr_spectra(self.h, _dptr(kn), _dptr(es), _dptr(ed),
                                            ec.ctypes.data_as(C.POINTER(C.c_int64))))
         return kn, es, ed, ec
+
+    def profile(self, nsteps: int):
+        """Per-kernel device time over nsteps iterations (CUDA events around every launch)."""
+        stats = (CKernelStat * 64)()
+        n = C.c_int32()
+        self._check(self.lib.bastr_profile(self.h, nsteps, stats, 64, C.byref(n)))
+        return [{"name": stats[i].name.decode(), "launches": stats[i].launches,
+                 "total_ms": stats[i].total_ms, "bytes_per_launch": stats[i].bytes_per_launch}
+                for i in range(min(n.value, 64))]
 
     def fft(self, array: np.ndarray, direction: int) -> np.ndarray:
         """fft2d/fft3d (direction -1, scaled 1/N) or ifft2d/ifft3d (+1) of a full complex grid."""

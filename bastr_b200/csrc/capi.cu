@@ -68,6 +68,13 @@ struct bastr_handle {
     int64_t batch_n0 = 0;      // nstep and time at the start of that batch
     double batch_t0 = 0.0;
     Twiddles tw[3];            // per axis x, y, z
+    size_t n_disk = 0;         // kept modes with |k| < K (state entries the spectra kernel reads, per component)
+    // per-launch profiling (bastr_profile): CUDA events around every launch
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    struct ProfRec { const char* name; size_t ev; double bytes; };
+    std::vector<ProfRec> prof;
     std::vector<double> kn;
     std::vector<int64_t> ecount;
 };
@@ -93,6 +100,38 @@ int fail(bastr_handle* h, int code, const char* fmt, ...) {
     } while (0)
 
 bool is_pow2(int n) { return n >= 16 && n <= 2048 && (n & (n - 1)) == 0; }
+
+// Brackets one kernel launch with CUDA events when profiling is on; `bytes` is the launch's
+// algorithmic traffic (unique global reads plus writes of its inputs and outputs).
+struct ProfScope {
+    bastr_handle* h;
+    size_t ev = 0;
+    bool on = false;
+    ProfScope(bastr_handle* hh, const char* name, double bytes) : h(hh) {
+        if (!h->prof_on || h->ev_used + 2 > h->ev_pool.size()) return;
+        ev = h->ev_used;
+        h->ev_used += 2;
+        on = true;
+        cudaEventRecord(h->ev_pool[ev], h->stream);
+        h->prof.push_back({name, ev, bytes});
+    }
+    ~ProfScope() {
+        if (on) cudaEventRecord(h->ev_pool[ev + 1], h->stream);
+    }
+};
+
+// Global traffic of the state-side reads/writes of one epilogue over n entries.
+double epi_bytes(int epi, bool from_u0, double n, double cs) {
+    switch (epi) {
+        case EPI_STORE: return n * 16;
+        case EPI_RK1: return n * 16 + 2 * n * cs;
+        case EPI_RK2: return 3 * n * cs + n * 16 + 2 * n * cs;
+        case EPI_RK3: return 2 * n * cs + n * 16 + n * 16;
+        case EPI_CN_MID: return from_u0 ? n * 16 + n * cs : 2 * n * cs + n * 16;
+        case EPI_CN_LAST: return n * cs + 2 * n * 16;
+    }
+    return 0;
+}
 
 template <typename T> const cplx<T>* twp(const Twiddles& t);
 template <> const cplx<double>* twp<double>(const Twiddles& t) { return t.d64; }
@@ -139,6 +178,9 @@ cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
         auto k = k2d_yinv<T, TIN, NN, SET>;
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
+        const double K_ = h->g.K;
+        ProfScope ps(h, SET == YI_VG ? "k2d_yinv_vg" : "k2d_yinv",
+                     K_ * h->g.KY * 2 * sizeof(cplx<TIN>) + (double)h->g.ny * K_ * P::F * sizeof(cplx<T>));
         k<<<h->g.K, P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g,
                                                   twp<T>(h->tw[1]));
     });
@@ -153,6 +195,10 @@ cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const 
         auto k = k2d_xpass<T, NN, MODE>;
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
+        const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.K, phys = 2.0 * h->g.nx * h->g.ny * 8;
+        const double b = MODE == XM_RHS ? mix * 6 * cs : MODE == XM_RHS_VG ? mix * 9 * cs
+                       : MODE == XM_TO_PHYS ? mix * 2 * cs + phys : phys + mix * 2 * cs;
+        ProfScope ps(h, MODE == XM_RHS_VG ? "k2d_xpass_vg" : MODE == XM_RHS ? "k2d_xpass" : "k2d_xpass_state", b);
         k<<<h->g.ny / P::BR, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg,
                                                           h->g, twp<T>(h->tw[0]));
     });
@@ -166,6 +212,9 @@ cudaError_t l2_yfwd(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0)
         auto k = k2d_yfwd<T, NN, EPI>;
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
+        const double cs = sizeof(cplx<T>);
+        ProfScope ps(h, "k2d_yfwd", (double)h->g.K * h->g.ny * 2 * cs +
+                                    epi_bytes(EPI, from_u0, (double)h->g.K * h->g.KY * 2, cs));
         k<<<h->g.K, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]));
     });
     return cudaGetLastError();
@@ -229,6 +278,9 @@ cudaError_t l3_zinv(bastr_handle* h, const void* S, void* MA, int ftot) {
         auto k = k3d_zinv<T, TIN, NN, SET>;
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
+        const double lines = (double)h->g.K * h->g.KY;
+        ProfScope ps(h, SET == ZI_VG ? "k3d_zinv_vg" : "k3d_zinv",
+                     lines * h->g.KZ * 3 * sizeof(cplx<TIN>) + lines * h->g.nz * P::F * sizeof(cplx<T>));
         k<<<cdiv(h->g.K * h->g.KY, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot,
                                                                          h->g, twp<T>(h->tw[2]));
     });
@@ -242,6 +294,9 @@ cudaError_t l3_yinv(bastr_handle* h, const void* MA, void* MB) {
         auto k = k3d_yinv<T, NN, SET>;
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
+        const double cs = sizeof(cplx<T>);
+        ProfScope ps(h, SET == YB_RHS_VG ? "k3d_yinv_vg" : "k3d_yinv",
+                     (double)h->g.K * h->g.nz * (h->g.KY * P::FIN + h->g.ny * P::F) * cs);
         k<<<cdiv(h->g.K * h->g.nz, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, (cplx<T>*)MB, h->g,
                                                                          twp<T>(h->tw[1]));
     });
@@ -255,6 +310,11 @@ cudaError_t l3_xpass(bastr_handle* h, const void* MB, void* MC, const double* pi
         auto k = k3d_xpass<T, NN, MODE>;
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
+        const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.nz * h->g.K;
+        const double phys = 3.0 * h->g.nx * h->g.ny * h->g.nz * 8;
+        const double b = MODE == X3_RHS ? mix * 12 * cs : MODE == X3_RHS_VG ? mix * 16 * cs
+                       : MODE == X3_TO_PHYS ? mix * 3 * cs + phys : phys + mix * 3 * cs;
+        ProfScope ps(h, MODE == X3_RHS_VG ? "k3d_xpass_vg" : MODE == X3_RHS ? "k3d_xpass" : "k3d_xpass_state", b);
         k<<<h->g.ny * h->g.nz / P::BR, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg,
                                                                        h->g, twp<T>(h->tw[0]));
     });
@@ -268,6 +328,7 @@ cudaError_t l3_yfwd(bastr_handle* h, const void* MC, void* MD) {
         auto k = k3d_yfwd<T, NN>;
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
+        ProfScope ps(h, "k3d_yfwd", (double)h->g.K * h->g.nz * (h->g.ny + h->g.KY) * 3 * sizeof(cplx<T>));
         k<<<cdiv(h->g.K * h->g.nz, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MC, (cplx<T>*)MD, h->g,
                                                                          twp<T>(h->tw[1]));
     });
@@ -281,6 +342,8 @@ cudaError_t l3_zfwd(bastr_handle* h, const void* MD, StageIO<T> io, int from_u0)
         auto k = k3d_zfwd<T, NN, EPI>;
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
+        const double cs = sizeof(cplx<T>), lines = (double)h->g.K * h->g.KY;
+        ProfScope ps(h, "k3d_zfwd", lines * h->g.nz * 3 * cs + epi_bytes(EPI, from_u0, lines * h->g.KZ * 3, cs));
         k<<<cdiv(h->g.K * h->g.KY, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MD, io, from_u0, h->g,
                                                                          twp<T>(h->tw[2]));
     });
@@ -394,8 +457,12 @@ cudaError_t launch_rhs(bastr_handle* h, int epi, bool from_u0, bool vg) {
 }
 
 cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out) {
+    {
+    ProfScope ps(h, "k_spectra", (double)h->n_disk * h->g.d * 16);
     if (h->g.d == 2) k_spectra<2, 256><<<h->nshell, 256, 0, h->stream>>>(h->u0, h->g, h->shell);
     else k_spectra<3, 256><<<h->nshell, 256, 0, h->stream>>>(h->u0, h->g, h->shell);
+    }
+    ProfScope ps(h, "k_spectra_final", (double)h->nshell * 32);
     k_spectra_final<256><<<1, 256, 0, h->stream>>>(h->shell, h->nshell, h->allkmax, rec, shells_out);
     return cudaGetLastError();
 }
@@ -404,13 +471,19 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec) {
     const int m = h->p.forcemethod;
     if (m == 0) return cudaSuccess;
     if (m == 1 || m == 5) {
+        ProfScope ps(h, "k_sum_partials", (double)h->n_en_blocks * 8);
         k_sum_partials<256><<<1, 256, 0, h->stream>>>(h->en_part, h->n_en_blocks, 1.0, rec, R_ENERGY);
     }
     if (m == 1) {
-        k_force_linear_factor<<<1, 32, 0, h->stream>>>(rec, h->p.target_energy);
+        {
+            ProfScope ps(h, "k_force_linear_factor", 16);
+            k_force_linear_factor<<<1, 32, 0, h->stream>>>(rec, h->p.target_energy);
+        }
+        ProfScope ps(h, "k_scale_state", (double)h->n_state * 32);
         k_scale_state<<<148 * 4, 256, 0, h->stream>>>(h->u0, h->n_state, rec);
     } else {
         const int proj = (m == 5 && h->g.d == 2 && h->p.lprojectd) ? 1 : 0;
+        ProfScope ps(h, "k_force_band", 0);
         if (h->g.d == 2)
             k_force_band<2, 256><<<1, 256, 0, h->stream>>>(h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec);
         else
@@ -428,7 +501,10 @@ cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
     if (h->p.timemethod == 1) {
         e = launch_rhs(h, EPI_RK1, true, vg);
         if (e != cudaSuccess) return e;
-        if (vg) k_velgrad_final<256><<<1, 256, 0, h->stream>>>(h->vg_part, h->n_vg_blocks, h->g, rec);
+        if (vg) {
+            ProfScope ps(h, "k_velgrad_final", (double)h->n_vg_blocks * 64);
+            k_velgrad_final<256><<<1, 256, 0, h->stream>>>(h->vg_part, h->n_vg_blocks, h->g, rec);
+        }
         e = launch_rhs(h, EPI_RK2, false, false);
         if (e != cudaSuccess) return e;
         e = launch_rhs(h, EPI_RK3, false, false);
@@ -437,7 +513,10 @@ cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
         for (int s = 1; s <= 6; ++s) {
             e = launch_rhs(h, s == 6 ? EPI_CN_LAST : EPI_CN_MID, s == 1, vg && s == 1);
             if (e != cudaSuccess) return e;
-            if (vg && s == 1) k_velgrad_final<256><<<1, 256, 0, h->stream>>>(h->vg_part, h->n_vg_blocks, h->g, rec);
+            if (vg && s == 1) {
+                ProfScope ps(h, "k_velgrad_final", (double)h->n_vg_blocks * 64);
+                k_velgrad_final<256><<<1, 256, 0, h->stream>>>(h->vg_part, h->n_vg_blocks, h->g, rec);
+            }
         }
     }
     return launch_forcing(h, rec);
@@ -521,6 +600,7 @@ void free_all(bastr_handle* h) {
         if (t.d64) cudaFree(t.d64);
         if (t.d32) cudaFree(t.d32);
     }
+    for (cudaEvent_t ev : h->ev_pool) cudaEventDestroy(ev);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -648,6 +728,19 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
         CK(cudaMemcpy(h->tw[a].d32, t32.data(), ns[a] * sizeof(float2), cudaMemcpyHostToDevice));
     }
     host_shells(h);
+    {
+        const long long K2 = (long long)K * K;
+        size_t nd = 0;
+        for (int kx = 0; kx < K; ++kx)
+            for (int ky = -(K - 1); ky <= K - 1; ++ky) {
+                const long long r = (long long)kx * kx + (long long)ky * ky;
+                if (r >= K2) continue;
+                if (d == 2) { ++nd; continue; }
+                for (int kz = -(K - 1); kz <= K - 1; ++kz)
+                    if (r + (long long)kz * kz < K2) ++nd;
+            }
+        h->n_disk = nd;
+    }
     h->launches_per_step = count_launches(h, p->velgrad_every > 0);
     CK(cudaDeviceSynchronize());
     return BASTR_OK;
@@ -796,6 +889,48 @@ int bastr_fft(bastr_handle* h, double* array, int32_t dir) {
     if (!h || !array || (dir != 1 && dir != -1)) return fail(h, BASTR_E_INVALID, "bastr_fft arguments");
     CK(cudaSetDevice(h->device));
     return full_fft(h, array, dir);
+}
+
+int bastr_profile(bastr_handle* h, int32_t nsteps, bastr_kernel_stat* stats, int32_t max_stats, int32_t* n_stats) {
+    if (!h || nsteps < 1 || nsteps > kChunk) return fail(h, BASTR_E_INVALID, "bastr_profile: 1..%d steps", kChunk);
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    CK(cudaSetDevice(h->device));
+    const size_t need = (size_t)2 * nsteps * (h->launches_per_step + 4);
+    while (h->ev_pool.size() < need) {
+        cudaEvent_t ev;
+        CK(cudaEventCreate(&ev));
+        h->ev_pool.push_back(ev);
+    }
+    h->ev_used = 0;
+    h->prof.clear();
+    h->prof_on = true;
+    const int r = bastr_step_async(h, nsteps);
+    h->prof_on = false;
+    if (r) return r;
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<std::string> names;
+    std::vector<double> tot, bytes;
+    std::vector<int> cnt;
+    for (const auto& pr : h->prof) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, h->ev_pool[pr.ev], h->ev_pool[pr.ev + 1]));
+        size_t i = 0;
+        while (i < names.size() && names[i] != pr.name) ++i;
+        if (i == names.size()) { names.push_back(pr.name); tot.push_back(0); bytes.push_back(0); cnt.push_back(0); }
+        tot[i] += ms;
+        bytes[i] += pr.bytes;
+        cnt[i] += 1;
+    }
+    const int n = (int)std::min<size_t>(names.size(), (size_t)std::max(max_stats, 0));
+    for (int i = 0; i < n && stats; ++i) {
+        memset(stats[i].name, 0, sizeof stats[i].name);
+        strncpy(stats[i].name, names[i].c_str(), sizeof stats[i].name - 1);
+        stats[i].launches = cnt[i];
+        stats[i].total_ms = tot[i];
+        stats[i].bytes_per_launch = bytes[i] / cnt[i];
+    }
+    if (n_stats) *n_stats = (int32_t)names.size();
+    return BASTR_OK;
 }
 
 int bastr_set_stream(bastr_handle* h, void* s) {

@@ -23,6 +23,9 @@
  * bastr_fft                   fft2d/fft3d/ifft2d/ifft3d (fftwlink.F90:324-368), in place on a
  *                             full complex(8) grid, for Bastrpp-style callers
  * bastr_destroy               deallocation (fftwlink.F90:469-490)
+ * bastr_profile, bastr_info,  no reference counterpart: per-kernel timing and introspection
+ *   bastr_step_async/records,  for measurement; asynchronous stepping and stream control
+ *   bastr_set_stream, bastr_sync
  * bastr_last_error            the reference's `stop 'message'` text, as a return value
  *
  * Layout: fields are real(8) arrays in Fortran order u(1:ia,1:ja[,1:ka]), x fastest,
@@ -115,6 +118,18 @@ BASTR_API int bastr_sync(bastr_handle* h);
 
 /* Introspection: allkmax, kernels launched per step, device bytes held. */
 BASTR_API int bastr_info(bastr_handle* h, int32_t* allkmax, int32_t* launches_per_step, int64_t* device_bytes);
+
+/* Per-kernel timing: runs nsteps (1..256) iterations with CUDA events around every launch and
+ * returns, per kernel, launches, total device time and algorithmic bytes per launch (unique
+ * global reads plus writes of its inputs and outputs).  The state advances by nsteps. */
+typedef struct bastr_kernel_stat {
+    char name[48];
+    int32_t launches;
+    double total_ms;
+    double bytes_per_launch;
+} bastr_kernel_stat;
+BASTR_API int bastr_profile(bastr_handle* h, int32_t nsteps, bastr_kernel_stat* stats, int32_t max_stats,
+                            int32_t* n_stats);
 
 /* Copies the message of the last failed call into buf (NUL-terminated); returns its length. */
 BASTR_API int bastr_last_error(bastr_handle* h, char* buf, int32_t n);

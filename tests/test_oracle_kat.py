@@ -1,0 +1,185 @@
+"""Known-answer tests that pin the CPU oracle (the reference ships no tests or fixtures, so the
+restatement is pinned by analytic results):
+
+* transforms: normalisation and sign of fft/ifft (fftwlink.F90:324-368) on single modes;
+* derivatives and the right-hand side of a single mode (solution.F90:816-863);
+* dealias mask and projection (tool.F90:175-270);
+* Parseval: Es + Ed = mean(|u|^2)/2 (solution.F90:930-1016);
+* linear viscous decay exp(-nu k^2 t) of a small-amplitude mode;
+* the 1-D viscous Burgers equation embedded in 2D and 3D against the Cole-Hopf solution;
+* the log format (1X,I20,n(1X,E20.13E2)) of listwrite (utility.F90:87-164).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.bastr_oracle import (Oracle, Params, dealias_mask, fortran_e20_13, generate_wave, kint,
+                                 listwrite_line, miucal)
+
+
+def grid(n):
+    return 2 * np.pi * np.arange(n) / n
+
+
+def test_miucal_is_one_at_unit_temperature():
+    assert miucal(1.0, 273.15) == pytest.approx(1.0, abs=1e-15)
+    assert Params(ia=16, ja=16, reynolds=5000.0).nu == pytest.approx(2e-4, rel=1e-15)
+    assert Params(ia=16, ja=16, reynolds=0.0).nu == 0.0
+
+
+def test_wavenumbers_and_nyquist_sign():
+    k1, k2 = generate_wave(Params(ia=8, ja=8))
+    assert list(k1[0]) == [0, 1, 2, 3, 4, -3, -2, -1]   # Nyquist index carries +ia/2
+    assert list(k2[:, 0]) == [0, 1, 2, 3, 4, -3, -2, -1]
+
+
+def test_kint_rounds_half_away_from_zero():
+    assert list(kint(np.array([0.0, 0.49, 0.5, 1.5, 2.5, 2.49]))) == [0, 0, 1, 2, 3, 2]
+
+
+def test_fft_normalisation_and_sign():
+    p = Params(ia=16, ja=16)
+    o = Oracle(p, [np.zeros(p.shape)] * 2)
+    x = grid(16)[None, :].repeat(16, 0)
+    f = o.fft(np.cos(3 * x) + 2 * np.sin(2 * x))
+    assert f[0, 3] == pytest.approx(0.5) and f[0, 13] == pytest.approx(0.5)
+    assert f[0, 2] == pytest.approx(-1j) and f[0, 14] == pytest.approx(1j)   # e^{-ikx} convention
+    assert np.allclose(o.ifft(f).real, np.cos(3 * x) + 2 * np.sin(2 * x))
+
+
+def test_dealias_mask_counts():
+    p = Params(ia=12, ja=12)
+    k1, k2 = generate_wave(p)
+    kk = np.sqrt(k1 ** 2 + k2 ** 2)
+    keep = dealias_mask(p, kk)
+    # cutoff floor(12/3) = 4: kept modes are the integer points strictly inside radius 4
+    expect = sum(1 for a in range(-5, 7) for b in range(-5, 7) if a * a + b * b < 16)
+    assert keep.sum() == expect
+
+
+def test_single_mode_rhs():
+    """u = (sin x, 0): u_t = -u u_x + nu u_xx = -sin(2x)/2 - nu sin x."""
+    n = 16
+    p = Params(ia=n, ja=n, reynolds=100.0)
+    x = grid(n)[None, :].repeat(n, 0)
+    u = [np.sin(x), np.zeros_like(x)]
+    for proj in (False, True):
+        p.lprojectd = proj
+        o = Oracle(p, u)
+        ut, _ = o.compute_ut([o.fft(c) for c in o.u])
+        assert np.allclose(ut[0].real, -0.5 * np.sin(2 * x) - p.nu * np.sin(x), atol=1e-14)
+        assert np.allclose(ut[1].real, 0.0, atol=1e-14)
+
+
+def test_projection_keeps_only_dilatational_part():
+    n = 16
+    p = Params(ia=n, ja=n, lprojectd=True)
+    x = grid(n)[None, :].repeat(n, 0)
+    y = x.T
+    # solenoidal (sin y, 0) + dilatational (sin x, 0)
+    o = Oracle(p, [np.sin(y) + np.sin(x), np.zeros((n, n))])
+    s = o.projection([o.fft(c) for c in o.u])
+    assert np.allclose(o.ifft(s[0]).real, np.sin(x), atol=1e-14)
+    assert np.allclose(o.ifft(s[1]).real, 0.0, atol=1e-14)
+
+
+def test_parseval_and_single_mode_spectra():
+    n = 32
+    p = Params(ia=n, ja=n, kmax=10)
+    x = grid(n)[None, :].repeat(n, 0)
+    y = x.T
+    o = Oracle(p, [np.cos(3 * x), np.cos(3 * x)])   # (cos 3x, cos 3x): d-part in x, s-part in y
+    sp = o.spectra_compute([o.fft(c) for c in o.u])
+    assert sp["Ed"][3] == pytest.approx(0.25, abs=1e-14)
+    assert sp["Es"][3] == pytest.approx(0.25, abs=1e-14)
+    assert sp["Esspe"] + sp["Edspe"] == pytest.approx(0.5, abs=1e-14)
+    rng = np.random.default_rng(0)
+    o = Oracle(p, [rng.standard_normal((n, n)), rng.standard_normal((n, n))])
+    o.initial_dealias()
+    sp = o.spectra_compute([o.fft(c) for c in o.u])
+    # the k = 0 mode carries no Es/Ed (|k| <= dk/2, solution.F90:957-972)
+    mean_sq = np.mean(o.u[0]) ** 2 + np.mean(o.u[1]) ** 2
+    assert sp["Esspe"] + sp["Edspe"] == pytest.approx(np.mean(o.u[0] ** 2 + o.u[1] ** 2) / 2 - mean_sq / 2,
+                                                      rel=1e-13)
+    # shell counts: Ecount(s) = #integer points with nint(|k|) = s
+    for s in range(1, 11):
+        cnt = sum(1 for a in range(-16, 16) for b in range(-16, 16)
+                  if math.floor(math.sqrt(a * a + b * b) + 0.5) == s)
+        assert sp["Ecount"][s] == cnt
+
+
+def test_linear_viscous_decay():
+    n, eps = 32, 1e-9
+    p = Params(ia=n, ja=n, reynolds=50.0, deltat=1e-3)
+    x = grid(n)[None, :].repeat(n, 0)
+    y = x.T
+    u = [eps * np.sin(3 * x) * np.cos(2 * y), eps * np.cos(3 * x) * np.sin(2 * y)]
+    o = Oracle(p, u)
+    o.initial_dealias()
+    for _ in range(50):
+        o.step_once(False)
+    decay = math.exp(-p.nu * 13 * 50 * p.deltat)
+    assert np.allclose(o.u[0], u[0] * decay, atol=eps * 1e-6)
+    assert np.allclose(o.u[1], u[1] * decay, atol=eps * 1e-6)
+
+
+def cole_hopf(x, t, nu, nterms=60):
+    """Exact 1-D viscous Burgers solution for u0 = sin x (Cole 1951, Hopf 1950)."""
+    from scipy.special import ive
+    a = 1.0 / (2.0 * nu)
+    num = np.zeros_like(x)
+    den = np.full_like(x, ive(0, a))
+    for m in range(1, nterms):
+        w = ive(m, a) * math.exp(-nu * m * m * t)
+        num += 4.0 * nu * m * w * np.sin(m * x)
+        den += 2.0 * w * np.cos(m * x)
+    return num / den
+
+
+@pytest.mark.parametrize("proj", [False, True])
+def test_cole_hopf_2d(proj):
+    n = 64
+    p = Params(ia=n, ja=n, reynolds=10.0, deltat=1e-3, lprojectd=proj)
+    x = grid(n)[None, :].repeat(n, 0)
+    o = Oracle(p, [np.sin(x), np.zeros((n, n))])
+    o.initial_dealias()
+    for _ in range(100):
+        o.step_once(False)
+    exact = cole_hopf(grid(n), 0.1, p.nu)
+    assert np.max(np.abs(o.u[0] - exact[None, :])) < 1e-7
+    assert np.max(np.abs(o.u[1])) < 1e-14
+
+
+def test_cole_hopf_3d_cn():
+    n = 32
+    p = Params(ia=n, ja=n, ka=n, reynolds=10.0, deltat=5e-4, timemethod=2)
+    x = np.broadcast_to(grid(n)[None, None, :], (n, n, n))
+    o = Oracle(p, [np.sin(x), np.zeros((n, n, n)), np.zeros((n, n, n))])
+    o.initial_dealias()
+    for _ in range(40):
+        o.step_once(False)
+    exact = cole_hopf(grid(n), 40 * p.deltat, p.nu)
+    # Crank-Nicolson fixed point: second order in time
+    assert np.max(np.abs(o.u[0] - exact[None, None, :])) < 1e-6
+
+
+def test_band_forcing_reaches_target():
+    n = 32
+    p = Params(ia=n, ja=n, forcemethod=2, forcek=3, target_energy=0.3, deltat=1e-4)
+    rng = np.random.default_rng(1)
+    o = Oracle(p, [rng.standard_normal((n, n)), rng.standard_normal((n, n))])
+    o.initial_dealias()
+    rec, _ = o.step_once(False)
+    factor, E = rec.forcing
+    # after forcing, mean(f^2) over the band equals target (band energy rescaled by (1+factor)^2)
+    assert E * (1 + factor) ** 2 == pytest.approx(0.3, rel=1e-12)
+
+
+def test_listwrite_format():
+    assert fortran_e20_13(1.0) == " 0.1000000000000E+01"
+    assert fortran_e20_13(-0.075) == "-0.7500000000000E-01"
+    assert fortran_e20_13(0.0) == " 0.0000000000000E+00"
+    assert fortran_e20_13(1.5e-120) == " 0.1500000000000-119"
+    line = listwrite_line(3, 3e-4, 1.0, 2.0)
+    assert line == "                    3  0.3000000000000E-03  0.1000000000000E+01  0.2000000000000E+01"
