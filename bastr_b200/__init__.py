@@ -38,7 +38,9 @@ EXPORTED = [
     "bastr_create", "bastr_destroy", "bastr_set_state", "bastr_get_state", "bastr_set_counters",
     "bastr_get_counters", "bastr_step", "bastr_step_async", "bastr_step_records", "bastr_spectra",
     "bastr_fft", "bastr_set_stream", "bastr_sync", "bastr_info", "bastr_last_error", "bastr_profile",
+    "bastr_spectra_noalloc",
 ]
+BASTR_E_TOO_LARGE = -6
 
 
 class BastrError(RuntimeError):
@@ -99,6 +101,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_info.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     lib.bastr_last_error.argtypes = [P, C.c_char_p, C.c_int32]
     lib.bastr_profile.argtypes = [P, C.c_int32, C.POINTER(CKernelStat), C.c_int32, C.POINTER(C.c_int32)]
+    lib.bastr_spectra_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P, P, P]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib

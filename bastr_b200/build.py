@@ -13,8 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbastr_gpu.so")
-SOURCES = ["capi.cu"]
-DEPS = ["capi.cu", "pass2d.cu", "pass3d.cu", "diag.cu", "fft_engine.cuh", "solver.cuh"]
+SOURCES = ["capi.cu", "noalloc.cu"]
+DEPS = ["capi.cu", "pass2d.cu", "pass3d.cu", "diag.cu", "noalloc.cu", "fft_engine.cuh", "solver.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

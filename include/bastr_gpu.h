@@ -131,6 +131,27 @@ typedef struct bastr_kernel_stat {
 BASTR_API int bastr_profile(bastr_handle* h, int32_t nsteps, bastr_kernel_stat* stats, int32_t max_stats,
                             int32_t* n_stats);
 
+/* Shell spectra of a caller-owned spectrum, allocating nothing.  No counterpart in the reference:
+ * it serves callers that keep their spectra in their own device memory and cannot let a library
+ * call cudaMalloc (GPU memory owned by CUDA Fortran / OpenACC data regions of a post-processing
+ * driver, or a memory-capped pool), so they cannot create a handle, which allocates.
+ *   d_u1spe, d_u2spe[, d_u3spe]: device arrays of ia*ja*max(ka,1) complex(8) values (re, im
+ *       interleaved, x fastest), the forward-normalised spectra that fft2d/fft3d produce;
+ *   d_Es, d_Ed: device arrays of allkmax+1 doubles (allkmax = min(ia/3, kmax)), shells 0..allkmax;
+ *   d_totals (may be NULL): 4 doubles Esspe, Edspe, k2Edspe, kMEdspe over every mode.
+ * The only workspace is a fixed 128 KiB device array inside the library (BASTR_NOALLOC_MAX_SHELLS
+ * shells x 4 doubles), held by every GPU that loads the library until the process exits; grids
+ * with nint(|k|max) + 1 > BASTR_NOALLOC_MAX_SHELLS are rejected with BASTR_E_TOO_LARGE.  The first
+ * call on a device looks up that array's device address, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams or host threads) race
+ * and must be serialised by the caller.  Each call writes every slot it reads, so no clearing is
+ * needed between calls.  Runs on `stream` (NULL: legacy default stream), does not synchronise. */
+#define BASTR_NOALLOC_MAX_SHELLS 4096
+#define BASTR_E_TOO_LARGE (-6)
+BASTR_API int bastr_spectra_noalloc(int32_t ia, int32_t ja, int32_t ka, int32_t kmax,
+                                    const double* d_u1spe, const double* d_u2spe, const double* d_u3spe,
+                                    double* d_Es, double* d_Ed, double* d_totals, void* stream);
+
 /* Copies the message of the last failed call into buf (NUL-terminated); returns its length. */
 BASTR_API int bastr_last_error(bastr_handle* h, char* buf, int32_t n);
 
