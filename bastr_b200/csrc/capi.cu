@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <set>
 #include <string>
@@ -69,6 +70,12 @@ struct bastr_handle {
     double batch_t0 = 0.0;
     Twiddles tw[3];            // per axis x, y, z
     size_t n_disk = 0;         // kept modes with |k| < K (state entries the spectra kernel reads, per component)
+    // shell mode lists for the spectra (CSR): modes grouped by shell, cut into work items
+    int* sp_modes = nullptr;
+    int* sp_item_lo = nullptr;   // [n_items + 1]
+    int* sp_shell_item = nullptr; // [nshell + 1]
+    double* sp_item_part = nullptr;
+    int n_items = 0;
     // per-launch profiling (bastr_profile): CUDA events around every launch
     bool prof_on = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -137,21 +144,48 @@ template <typename T> const cplx<T>* twp(const Twiddles& t);
 template <> const cplx<double>* twp<double>(const Twiddles& t) { return t.d64; }
 template <> const cplx<float>* twp<float>(const Twiddles& t) { return t.d32; }
 
-// Enables the dynamic shared memory a kernel instance asks for, once per (device, kernel).
+// Enables the dynamic shared memory a kernel instance asks for and returns how many of its
+// blocks fit on one SM; both once per (device, kernel).
 std::mutex g_prep_mu;
-std::set<std::pair<int, const void*>> g_prepped;
-template <typename K> cudaError_t prep(K kernel, size_t smem) {
+std::map<std::pair<int, const void*>, int> g_prepped;
+int g_num_sms[64] = {};
+template <typename K> cudaError_t prep(K kernel, size_t smem, int nt = 0, int* blocks_per_sm = nullptr) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     const auto key = std::make_pair(dev, (const void*)kernel);
     std::lock_guard<std::mutex> lk(g_prep_mu);
-    if (g_prepped.count(key)) return cudaSuccess;
-    if (smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+    auto it = g_prepped.find(key);
+    if (it == g_prepped.end()) {
+        if (smem > 48 * 1024) {
+            e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        int nb = 1;
+        if (nt > 0) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, nt, smem);
+            if (e != cudaSuccess) return e;
+            if (nb < 1) nb = 1;
+        }
+        if (dev >= 0 && dev < 64 && g_num_sms[dev] == 0) {
+            e = cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return e;
+        }
+        it = g_prepped.emplace(key, nb).first;
     }
-    g_prepped.insert(key);
+    if (blocks_per_sm) *blocks_per_sm = it->second;
+    return cudaSuccess;
+}
+
+// Grid of a persistent pass: as many blocks as fit on the device, at most one per work item.
+template <typename K> cudaError_t persistent_grid(K kernel, size_t smem, int nt, int nitems, int* grid) {
+    int nb = 1;
+    cudaError_t e = prep(kernel, smem, nt, &nb);
+    if (e != cudaSuccess) return e;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int sms = (dev >= 0 && dev < 64 && g_num_sms[dev] > 0) ? g_num_sms[dev] : 148;
+    *grid = std::max(1, std::min(nitems, nb * sms));
     return cudaSuccess;
 }
 
@@ -168,21 +202,23 @@ template <typename K> cudaError_t prep(K kernel, size_t smem) {
         default: return cudaErrorInvalidValue;   \
     }
 
+int cdiv(int a, int b) { return (a + b - 1) / b; }
+
 // ---------------------------------------------------------------------------------------
 // 2D launches
 // ---------------------------------------------------------------------------------------
 template <typename T, typename TIN, int SET>
 cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
     SIZE_CASES(h->g.ny, {
-        using P = YInv2D<T, NN, SET>;
+        using P = YInv2D<T, TIN, NN, SET>;
         auto k = k2d_yinv<T, TIN, NN, SET>;
-        cudaError_t e = prep(k, P::SMEM);
+        int grid = 1;
+        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K, P::G), &grid);
         if (e != cudaSuccess) return e;
         const double K_ = h->g.K;
         ProfScope ps(h, SET == YI_VG ? "k2d_yinv_vg" : "k2d_yinv",
                      K_ * h->g.KY * 2 * sizeof(cplx<TIN>) + (double)h->g.ny * K_ * P::F * sizeof(cplx<T>));
-        k<<<h->g.K, P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g,
-                                                  twp<T>(h->tw[1]));
+        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[1]));
     });
     return cudaGetLastError();
 }
@@ -193,14 +229,16 @@ cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const 
     SIZE_CASES(h->g.nx, {
         using P = XPass2D<T, NN, MODE>;
         auto k = k2d_xpass<T, NN, MODE>;
-        cudaError_t e = prep(k, P::SMEM);
+        int grid = 1;
+        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.ny, P::G), &grid);
         if (e != cudaSuccess) return e;
+        if (MODE == XM_RHS_VG) h->n_vg_blocks = grid;
         const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.K, phys = 2.0 * h->g.nx * h->g.ny * 8;
         const double b = MODE == XM_RHS ? mix * 6 * cs : MODE == XM_RHS_VG ? mix * 9 * cs
                        : MODE == XM_TO_PHYS ? mix * 2 * cs + phys : phys + mix * 2 * cs;
         ProfScope ps(h, MODE == XM_RHS_VG ? "k2d_xpass_vg" : MODE == XM_RHS ? "k2d_xpass" : "k2d_xpass_state", b);
-        k<<<h->g.ny / P::BR, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg,
-                                                          h->g, twp<T>(h->tw[0]));
+        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg, h->g,
+                                                twp<T>(h->tw[0]));
     });
     return cudaGetLastError();
 }
@@ -210,26 +248,23 @@ cudaError_t l2_yfwd(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0)
     SIZE_CASES(h->g.ny, {
         using P = YFwd2D<T, NN>;
         auto k = k2d_yfwd<T, NN, EPI>;
-        cudaError_t e = prep(k, P::SMEM);
+        int grid = 1;
+        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K, P::G), &grid);
         if (e != cudaSuccess) return e;
+        if (io.energy_part) h->n_en_blocks = grid;
         const double cs = sizeof(cplx<T>);
         ProfScope ps(h, "k2d_yfwd", (double)h->g.K * h->g.ny * 2 * cs +
                                     epi_bytes(EPI, from_u0, (double)h->g.K * h->g.KY * 2, cs));
-        k<<<h->g.K, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]));
+        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]));
     });
     return cudaGetLastError();
-}
-
-template <typename T> int xpass_rows(bastr_handle* h, bool vg) {
-    (void)h;
-    return vg ? XPass2D<T, 64, XM_RHS_VG>::BR : XPass2D<T, 64, XM_RHS>::BR;
 }
 
 // One right-hand-side evaluation F(u_s) and its combination, 2D.
 template <typename T>
 cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
     cudaError_t e;
-    const int ftot = vg ? 7 : 4;
+    const int ftot = vg ? 8 : 4;
     if (from_u0) e = l2_yinv<T, double, YI_RHS>(h, h->u0, h->ma, ftot);
     else e = l2_yinv<T, T, YI_RHS>(h, h->us, h->ma, ftot);
     if (e != cudaSuccess) return e;
@@ -269,8 +304,6 @@ cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
         default: return cudaErrorInvalidValue;                \
     }
 
-int cdiv(int a, int b) { return (a + b - 1) / b; }
-
 template <typename T, typename TIN, int SET>
 cudaError_t l3_zinv(bastr_handle* h, const void* S, void* MA, int ftot) {
     SIZE_CASES3(h->g.nz, {
@@ -281,7 +314,7 @@ cudaError_t l3_zinv(bastr_handle* h, const void* S, void* MA, int ftot) {
         const double lines = (double)h->g.K * h->g.KY;
         ProfScope ps(h, SET == ZI_VG ? "k3d_zinv_vg" : "k3d_zinv",
                      lines * h->g.KZ * 3 * sizeof(cplx<TIN>) + lines * h->g.nz * P::F * sizeof(cplx<T>));
-        k<<<cdiv(h->g.K * h->g.KY, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot,
+        k<<<cdiv(h->g.K * h->g.KY, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot,
                                                                          h->g, twp<T>(h->tw[2]));
     });
     return cudaGetLastError();
@@ -297,7 +330,7 @@ cudaError_t l3_yinv(bastr_handle* h, const void* MA, void* MB) {
         const double cs = sizeof(cplx<T>);
         ProfScope ps(h, SET == YB_RHS_VG ? "k3d_yinv_vg" : "k3d_yinv",
                      (double)h->g.K * h->g.nz * (h->g.KY * P::FIN + h->g.ny * P::F) * cs);
-        k<<<cdiv(h->g.K * h->g.nz, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, (cplx<T>*)MB, h->g,
+        k<<<cdiv(h->g.K * h->g.nz, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, (cplx<T>*)MB, h->g,
                                                                          twp<T>(h->tw[1]));
     });
     return cudaGetLastError();
@@ -315,7 +348,7 @@ cudaError_t l3_xpass(bastr_handle* h, const void* MB, void* MC, const double* pi
         const double b = MODE == X3_RHS ? mix * 12 * cs : MODE == X3_RHS_VG ? mix * 16 * cs
                        : MODE == X3_TO_PHYS ? mix * 3 * cs + phys : phys + mix * 3 * cs;
         ProfScope ps(h, MODE == X3_RHS_VG ? "k3d_xpass_vg" : MODE == X3_RHS ? "k3d_xpass" : "k3d_xpass_state", b);
-        k<<<h->g.ny * h->g.nz / P::BR, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg,
+        k<<<cdiv(h->g.ny * h->g.nz, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg,
                                                                        h->g, twp<T>(h->tw[0]));
     });
     return cudaGetLastError();
@@ -329,7 +362,7 @@ cudaError_t l3_yfwd(bastr_handle* h, const void* MC, void* MD) {
         cudaError_t e = prep(k, P::SMEM);
         if (e != cudaSuccess) return e;
         ProfScope ps(h, "k3d_yfwd", (double)h->g.K * h->g.nz * (h->g.ny + h->g.KY) * 3 * sizeof(cplx<T>));
-        k<<<cdiv(h->g.K * h->g.nz, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MC, (cplx<T>*)MD, h->g,
+        k<<<cdiv(h->g.K * h->g.nz, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MC, (cplx<T>*)MD, h->g,
                                                                          twp<T>(h->tw[1]));
     });
     return cudaGetLastError();
@@ -344,7 +377,7 @@ cudaError_t l3_zfwd(bastr_handle* h, const void* MD, StageIO<T> io, int from_u0)
         if (e != cudaSuccess) return e;
         const double cs = sizeof(cplx<T>), lines = (double)h->g.K * h->g.KY;
         ProfScope ps(h, "k3d_zfwd", lines * h->g.nz * 3 * cs + epi_bytes(EPI, from_u0, lines * h->g.KZ * 3, cs));
-        k<<<cdiv(h->g.K * h->g.KY, P::L), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MD, io, from_u0, h->g,
+        k<<<cdiv(h->g.K * h->g.KY, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MD, io, from_u0, h->g,
                                                                          twp<T>(h->tw[2]));
     });
     return cudaGetLastError();
@@ -352,28 +385,28 @@ cudaError_t l3_zfwd(bastr_handle* h, const void* MD, StageIO<T> io, int from_u0)
 
 template <typename T> int zfwd_lines(int nz) {
     switch (nz) {
-        case 16: return ZFwd3D<T, 16>::L;
-        case 32: return ZFwd3D<T, 32>::L;
-        case 64: return ZFwd3D<T, 64>::L;
-        case 128: return ZFwd3D<T, 128>::L;
-        case 256: return ZFwd3D<T, 256>::L;
-        default: return ZFwd3D<T, 512>::L;
+        case 16: return ZFwd3D<T, 16>::G;
+        case 32: return ZFwd3D<T, 32>::G;
+        case 64: return ZFwd3D<T, 64>::G;
+        case 128: return ZFwd3D<T, 128>::G;
+        case 256: return ZFwd3D<T, 256>::G;
+        default: return ZFwd3D<T, 512>::G;
     }
 }
 template <typename T> int xpass3_rows_vg(int nx) {
     switch (nx) {
-        case 16: return XPass3D<T, 16, X3_RHS_VG>::BR;
-        case 32: return XPass3D<T, 32, X3_RHS_VG>::BR;
-        case 64: return XPass3D<T, 64, X3_RHS_VG>::BR;
-        case 128: return XPass3D<T, 128, X3_RHS_VG>::BR;
-        case 256: return XPass3D<T, 256, X3_RHS_VG>::BR;
-        default: return XPass3D<T, 512, X3_RHS_VG>::BR;
+        case 16: return XPass3D<T, 16, X3_RHS_VG>::G;
+        case 32: return XPass3D<T, 32, X3_RHS_VG>::G;
+        case 64: return XPass3D<T, 64, X3_RHS_VG>::G;
+        case 128: return XPass3D<T, 128, X3_RHS_VG>::G;
+        case 256: return XPass3D<T, 256, X3_RHS_VG>::G;
+        default: return XPass3D<T, 512, X3_RHS_VG>::G;
     }
 }
 
 int vg_blocks3d(bastr_handle* h) {
     const int br = h->fp32 ? xpass3_rows_vg<float>(h->g.nx) : xpass3_rows_vg<double>(h->g.nx);
-    return h->g.ny * h->g.nz / br;
+    return cdiv(h->g.ny * h->g.nz, br);
 }
 int en_blocks3d(bastr_handle* h) {
     const int l = h->fp32 ? zfwd_lines<float>(h->g.nz) : zfwd_lines<double>(h->g.nz);
@@ -457,13 +490,18 @@ cudaError_t launch_rhs(bastr_handle* h, int epi, bool from_u0, bool vg) {
 }
 
 cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out) {
-    {
-    ProfScope ps(h, "k_spectra", (double)h->n_disk * h->g.d * 16);
-    if (h->g.d == 2) k_spectra<2, 256><<<h->nshell, 256, 0, h->stream>>>(h->u0, h->g, h->shell);
-    else k_spectra<3, 256><<<h->nshell, 256, 0, h->stream>>>(h->u0, h->g, h->shell);
+    if (h->n_items > 0) {
+        ProfScope ps(h, "k_spectra", (double)h->n_disk * (h->g.d * 16 + 4));
+        if (h->g.d == 2)
+            k_spectra_items<2, 256><<<h->n_items, 256, 0, h->stream>>>(h->u0, h->g, h->sp_modes, h->sp_item_lo,
+                                                                       h->sp_item_part);
+        else
+            k_spectra_items<3, 256><<<h->n_items, 256, 0, h->stream>>>(h->u0, h->g, h->sp_modes, h->sp_item_lo,
+                                                                       h->sp_item_part);
     }
-    ProfScope ps(h, "k_spectra_final", (double)h->nshell * 32);
-    k_spectra_final<256><<<1, 256, 0, h->stream>>>(h->shell, h->nshell, h->allkmax, rec, shells_out);
+    ProfScope ps(h, "k_spectra_final", (double)h->n_items * 32);
+    k_spectra_items_final<256><<<1, 256, 0, h->stream>>>(h->sp_item_part, h->sp_shell_item, h->nshell,
+                                                          h->allkmax, rec, shells_out);
     return cudaGetLastError();
 }
 
@@ -593,7 +631,8 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
 
 void free_all(bastr_handle* h) {
     void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part,
-                    h->shell, h->rec, h->shells_dev};
+                    h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
+                    h->sp_item_part};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     for (auto& t : h->tw) {
@@ -688,12 +727,12 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     cudaError_t st = cudaSuccess;
     if (d == 2) {
         h->n_state = (size_t)K * g.KY * 2;
-        const size_t ma = std::max((size_t)g.ny * K * 7 * cs, (size_t)g.ny * K * 2 * sizeof(double2));
+        const size_t ma = std::max((size_t)g.ny * K * 8 * cs, (size_t)g.ny * K * 2 * sizeof(double2));
         const size_t mb = (size_t)K * g.ny * 2 * std::max(cs, sizeof(double2));
         dev_alloc(h, &h->ma, ma, st);
         dev_alloc(h, &h->mb, mb, st);
-        h->n_vg_blocks = g.ny / (h->fp32 ? xpass_rows<float>(h, true) : xpass_rows<double>(h, true));
-        h->n_en_blocks = K;
+        h->n_vg_blocks = 1;   // set by the launches (persistent grids)
+        h->n_en_blocks = 1;
     } else {
         h->n_state = (size_t)K * g.KY * g.KZ * 3;
         size_t ma, mb, mc;
@@ -708,8 +747,9 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     dev_alloc(h, &h->us, h->n_state * cs, st);
     dev_alloc(h, &h->acc, h->n_state * cs, st);
     dev_alloc(h, &h->phys, (size_t)d * npts * sizeof(double), st);
-    dev_alloc(h, &h->vg_part, (size_t)std::max(h->n_vg_blocks, 1) * 8 * sizeof(double), st);
-    dev_alloc(h, &h->en_part, (size_t)std::max(h->n_en_blocks, 1) * sizeof(double), st);
+    // partial sums: at most one per line group of the passes that produce them
+    dev_alloc(h, &h->vg_part, (size_t)std::max(g.ny * g.nz, 1) * 8 * sizeof(double), st);
+    dev_alloc(h, &h->en_part, (size_t)std::max(K * g.KY, 1) * sizeof(double), st);
     dev_alloc(h, &h->shell, (size_t)h->nshell * 4 * sizeof(double), st);
     dev_alloc(h, &h->rec, (size_t)kChunk * R_COUNT * sizeof(double), st);
     dev_alloc(h, &h->shells_dev, (size_t)kChunk * 2 * (h->allkmax + 1) * sizeof(double), st);
@@ -729,17 +769,49 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     }
     host_shells(h);
     {
+        // kept modes grouped by shell nint(|k|) (counting sort, increasing offset within a shell)
         const long long K2 = (long long)K * K;
-        size_t nd = 0;
-        for (int kx = 0; kx < K; ++kx)
-            for (int ky = -(K - 1); ky <= K - 1; ++ky) {
-                const long long r = (long long)kx * kx + (long long)ky * ky;
-                if (r >= K2) continue;
-                if (d == 2) { ++nd; continue; }
-                for (int kz = -(K - 1); kz <= K - 1; ++kz)
-                    if (r + (long long)kz * kz < K2) ++nd;
-            }
-        h->n_disk = nd;
+        const int KZ = g.KZ, KYv = g.KY;
+        std::vector<int> cnt(h->nshell + 1, 0);
+        auto shell_of = [](long long m) { return (int)std::floor(std::sqrt((double)m) + 0.5); };
+        auto each_mode = [&](auto&& fn) {
+            for (int kx = 0; kx < K; ++kx)
+                for (int kyi = 0; kyi < KYv; ++kyi) {
+                    const long long ky = kyi < K ? kyi : kyi - KYv;
+                    const long long r = (long long)kx * kx + ky * ky;
+                    if (r >= K2) continue;
+                    for (int kzi = 0; kzi < KZ; ++kzi) {
+                        const long long kz = d == 3 ? (kzi < K ? kzi : kzi - KZ) : 0;
+                        const long long m = r + kz * kz;
+                        if (m == 0 || m >= K2) continue;
+                        fn((int)(((long long)kx * KYv + kyi) * KZ + kzi), shell_of(m));
+                    }
+                }
+        };
+        each_mode([&](int, int sh) { cnt[sh + 1]++; });
+        for (int i = 1; i <= h->nshell; ++i) cnt[i] += cnt[i - 1];
+        std::vector<int> modes(cnt[h->nshell]);
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        each_mode([&](int idx, int sh) { modes[fill[sh]++] = idx; });
+        h->n_disk = modes.size() + 1;   // plus the k = 0 mode
+        constexpr int kItem = 2048;     // list entries per work item
+        std::vector<int> item_lo, shell_item(h->nshell + 1, 0);
+        for (int sh = 0; sh < h->nshell; ++sh) {
+            shell_item[sh] = (int)item_lo.size();
+            for (int a = cnt[sh]; a < cnt[sh + 1]; a += kItem) item_lo.push_back(a);
+        }
+        shell_item[h->nshell] = (int)item_lo.size();
+        h->n_items = (int)item_lo.size();
+        item_lo.push_back(cnt[h->nshell]);
+        dev_alloc(h, &h->sp_modes, std::max<size_t>(modes.size(), 1) * sizeof(int), st);
+        dev_alloc(h, &h->sp_item_lo, item_lo.size() * sizeof(int), st);
+        dev_alloc(h, &h->sp_shell_item, shell_item.size() * sizeof(int), st);
+        dev_alloc(h, &h->sp_item_part, (size_t)std::max(h->n_items, 1) * 4 * sizeof(double), st);
+        if (st != cudaSuccess) return fail(h, BASTR_E_CUDA, "device allocation failed: %s", cudaGetErrorString(st));
+        if (!modes.empty())
+            CK(cudaMemcpy(h->sp_modes, modes.data(), modes.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->sp_item_lo, item_lo.data(), item_lo.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->sp_shell_item, shell_item.data(), shell_item.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
     h->launches_per_step = count_launches(h, p->velgrad_every > 0);
     CK(cudaDeviceSynchronize());

@@ -20,6 +20,9 @@ enum RecSlot : int {
     R_COUNT = 16
 };
 
+// Largest kx range a 2D shell block enumerates (K <= 682 for grids up to 2048).
+constexpr int kSpectraMaxCols = 2048;
+
 __device__ __forceinline__ long long isqrt_floor(long long v) {
     if (v <= 0) return 0;
     long long r = (long long)sqrt((double)v);
@@ -87,14 +90,40 @@ __global__ void __launch_bounds__(NT) k_spectra(const double2* __restrict__ U0, 
     if (lo <= hi) {
         const int kmax = s < K - 1 ? s : K - 1;
         if constexpr (D == 2) {
+            // Flatten the shell: per kx the modes are ky in [a,b] and [-b,-a] (a > 0) so that
+            // consecutive threads read consecutive ky of one column.
+            __shared__ int off[kSpectraMaxCols + 1];
+            __shared__ int ka[kSpectraMaxCols], kb[kSpectraMaxCols];
             for (int kx = threadIdx.x; kx <= kmax; kx += NT) {
                 const long long rlo = lo - (long long)kx * kx, rhi = hi - (long long)kx * kx;
-                if (rhi < 0) continue;
-                const int a = (int)isqrt_ceil(rlo), b = (int)isqrt_floor(rhi);
-                for (int ky = a; ky <= b; ++ky) {
-                    spectra_mode<2>(U0, g, kx, ky, 0, acc);
-                    if (ky != 0) spectra_mode<2>(U0, g, kx, -ky, 0, acc);
+                int a = 0, b = -1;
+                if (rhi >= 0) {
+                    a = (int)isqrt_ceil(rlo);
+                    b = (int)isqrt_floor(rhi);
                 }
+                ka[kx] = a;
+                kb[kx] = b;
+                off[kx + 1] = b >= a ? 2 * (b - a + 1) - (a == 0 ? 1 : 0) : 0;
+            }
+            if (threadIdx.x == 0) off[0] = 0;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int kx = 1; kx <= kmax + 1; ++kx) off[kx] += off[kx - 1];
+            }
+            __syncthreads();
+            const int total = off[kmax + 1];
+            for (int idx = threadIdx.x; idx < total; idx += NT) {
+                int l = 0, r = kmax;   // last kx with off[kx] <= idx
+                while (l < r) {
+                    const int m = (l + r + 1) >> 1;
+                    if (off[m] <= idx) l = m; else r = m - 1;
+                }
+                const int kx = l;
+                const int rr = idx - off[kx];
+                const int a = ka[kx], b = kb[kx];
+                const int npos = b - a + 1;
+                const int ky = rr < npos ? a + rr : -((a == 0 ? 1 : a) + (rr - npos));
+                spectra_mode<2>(U0, g, kx, ky, 0, acc);
             }
         } else {
             const int ny2 = 2 * kmax + 1;
@@ -116,6 +145,73 @@ __global__ void __launch_bounds__(NT) k_spectra(const double2* __restrict__ U0, 
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) shell[(size_t)s * 4 + i] = acc[i];
+    }
+}
+
+// Shell sums from a precomputed mode list: `modes` holds the state offset (in modes) of every
+// kept mode with 0 < |k|^2 < K^2, grouped by shell nint(|k|) and in increasing offset within a
+// shell; work item i covers modes [item_lo[i], item_lo[i+1]) of one shell.  One block per item
+// writes its four partial sums; consecutive threads read consecutive list entries.
+template <int D, int NT>
+__global__ void __launch_bounds__(NT) k_spectra_items(const double2* __restrict__ U0, Geo g,
+                                                      const int* __restrict__ modes,
+                                                      const int* __restrict__ item_lo,
+                                                      double* __restrict__ item_part /* [items][4] */) {
+    __shared__ double scratch[4 * NT];
+    const int lo = item_lo[blockIdx.x], hi = item_lo[blockIdx.x + 1];
+    double acc[4] = {0, 0, 0, 0};
+    for (int i = lo + threadIdx.x; i < hi; i += NT) {
+        const int m = modes[i];
+        if constexpr (D == 2) {
+            const int kx = m / g.KY, kyi = m - kx * g.KY;
+            spectra_mode<2>(U0, g, kx, trunc_k(kyi, g.K, g.KY), 0, acc);
+        } else {
+            const int kzi = m % g.KZ, r = m / g.KZ;
+            const int kx = r / g.KY, kyi = r - kx * g.KY;
+            spectra_mode<3>(U0, g, kx, trunc_k(kyi, g.K, g.KY), trunc_k(kzi, g.K, g.KZ), acc);
+        }
+    }
+    block_sum<4, NT>(acc, scratch);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) item_part[(size_t)blockIdx.x * 4 + i] = acc[i];
+    }
+}
+
+// Per-shell sums of the work items (items of shell s are shell_item[s] .. shell_item[s+1]-1),
+// totals over all shells in fixed order, and the copy of shells 0..allkmax for the spect log.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_spectra_items_final(const double* __restrict__ item_part,
+                                                            const int* __restrict__ shell_item, int nshell,
+                                                            int allkmax, double* __restrict__ rec,
+                                                            double* __restrict__ shells_out) {
+    __shared__ double scratch[4 * NT];
+    double acc[4] = {0, 0, 0, 0};
+    for (int s = threadIdx.x; s < nshell; s += NT) {
+        double sh[4] = {0, 0, 0, 0};
+        for (int it = shell_item[s]; it < shell_item[s + 1]; ++it) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) sh[i] += item_part[(size_t)it * 4 + i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[i] += sh[i];
+        if (shells_out && s <= allkmax) {
+            shells_out[s] = sh[0];
+            shells_out[allkmax + 1 + s] = sh[1];
+        }
+    }
+    if (shells_out) {
+        for (int s = nshell + threadIdx.x; s <= allkmax; s += NT) {
+            shells_out[s] = 0.0;
+            shells_out[allkmax + 1 + s] = 0.0;
+        }
+    }
+    block_sum<4, NT>(acc, scratch);
+    if (threadIdx.x == 0) {
+        rec[R_ES] = acc[0];
+        rec[R_ED] = acc[1];
+        rec[R_K2ED] = acc[2];
+        rec[R_KMED] = acc[3];
     }
 }
 

@@ -6,109 +6,172 @@
 //             MA[y][kx][f]  f = g1,h1,g2,h2 (+ q1,q2,t when velocity-gradient statistics are due)
 //             g = IFFT_y(u^), h = IFFT_y(i ky u^), q = IFFT_y(ky^2 u^), t = IFFT_y(lap(theta)^)
 //   B  xpass: per y row, three (five) packed complex inverse x transforms give u, du/dx, du/dy
-//             (and lap u, lap theta) in physical space; the advective product
-//             N_i = -(u1 d1 u_i + u2 d2 u_i) is formed in registers and packed back into one
-//             forward x transform.  Output MB[kx][y][c].
+//             (and lap u, lap theta) in registers; the advective product
+//             N_i = -(u1 d1 u_i + u2 d2 u_i) is formed there and handed, still in registers,
+//             to one packed forward x transform.  Output MB[kx][y][c].
 //   C  yfwd : per kx column, forward y transforms, 1/N normalisation, truncation (= the
 //             spherical 2/3 dealias, tool.F90:175-194), viscous term -nu k^2 u^, dilatational
 //             projection (tool.F90:219-243) and the time-integrator combination.
 //
 // Two real fields share one complex transform (z = a + i b), so the six real inverse and two
 // real forward x transforms of the reference become three plus one complex transforms.
+//
+// Every pass is a persistent loop over groups of G contiguous lines, staged through shared memory
+// with cp.async (16-byte chunks, fully coalesced): as soon as a group's values sit in registers,
+// the copy of the next group is issued, so it lands while the current group is transformed.
+#include "regfft.cuh"
 #include "solver.cuh"
 
 namespace bastr {
 
-// ---------------------------------------------------------------------------------------
-// Pass A: inverse transforms along y of one kx column.
-// ---------------------------------------------------------------------------------------
-enum YInvSet : int { YI_STATE = 0, YI_RHS = 1, YI_VG = 2 };
+// Elements per thread per unit: 64 bytes of data per unit per thread in both precisions.
+template <typename T> struct EptOf { static constexpr int v = sizeof(T) == 8 ? 8 : 16; };
+template <int N, int EPT> constexpr int ept_fit() { return N < EPT ? N : EPT; }
+// Lines handled by one block: at least 128 threads per block.
+template <int NTR> constexpr int groups_per_block() { return NTR >= 128 ? 1 : 128 / NTR; }
 
-template <typename T, int NY, int SET> struct YInv2D {
-    static constexpr int F = SET == YI_STATE ? 2 : SET == YI_RHS ? 4 : 3;   // fields produced
-    static constexpr int F0 = SET == YI_VG ? 4 : 0;                          // offset in MA
-    static constexpr int US = padded_len(NY);
-    static constexpr int NT = pick_threads<T, F * NY>();
-    static constexpr size_t SMEM = (size_t)F * US * sizeof(cplx<T>);
-};
-
-template <typename T, typename TIN, int NY, int SET>
-__global__ void __launch_bounds__(YInv2D<T, NY, SET>::NT)
-k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Geo g,
-         const cplx<T>* __restrict__ tw) {
-    using P = YInv2D<T, NY, SET>;
-    constexpr int F = P::F, US = P::US, NT = P::NT;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
-    const int kx = blockIdx.x;
-    const int K = g.K, KY = g.KY;
-    const T kxt = (T)kx;
-    for (int p = threadIdx.x; p < NY; p += NT) {
-        cplx<T> v[F];
-#pragma unroll
-        for (int f = 0; f < F; ++f) v[f] = mk<T>(0, 0);
-        const int kyi = pos_trunc(p, K, KY, NY);
-        if (kyi >= 0) {
-            const T ky = (T)trunc_k(kyi, K, KY);
-            const size_t o = ((size_t)kx * KY + kyi) * 2;
-            cplx<T> a = cvt<cplx<TIN>, cplx<T>>(S[o]);
-            cplx<T> b = cvt<cplx<TIN>, cplx<T>>(S[o + 1]);
-            if constexpr (SET == YI_STATE) {
-                v[0] = a;
-                v[1] = b;
-            } else if constexpr (SET == YI_RHS) {
-                v[0] = a;
-                v[1] = cscale<T>(cmuli<T>(a), ky);
-                v[2] = b;
-                v[3] = cscale<T>(cmuli<T>(b), ky);
-            } else {
-                const T ky2 = ky * ky;
-                v[0] = cscale<T>(a, ky2);
-                v[1] = cscale<T>(b, ky2);
-                // lap(theta)^ = -i |k|^2 (kx u1^ + ky u2^)   (solution.F90:1131)
-                const T kk = kxt * kxt + ky2;
-                cplx<T> dv = cadd<T>(cscale<T>(a, kxt), cscale<T>(b, ky));
-                v[2] = cscale<T>(cmulni<T>(dv), kk);
-            }
-        }
-#pragma unroll
-        for (int f = 0; f < F; ++f) sm[f * US + pidx(p)] = v[f];
-    }
-    __syncthreads();
-    fft_run<T, NY, F, US, NT, true>(sm, tw);
-    const size_t rowstride = (size_t)K * ftot;
-    for (int e = threadIdx.x; e < NY * F; e += NT) {
-        const int y = e / F, f = e - y * F;
-        MA[(size_t)y * rowstride + (size_t)kx * ftot + P::F0 + f] = sm[f * US + pidx(y)];
+// Two adjacent complex values as one vector store.
+template <typename T> __device__ __forceinline__ void st2(cplx<T>* dst, cplx<T> a, cplx<T> b) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(dst) = make_float4(a.x, a.y, b.x, b.y);
+    } else {
+        dst[0] = a;
+        dst[1] = b;
     }
 }
 
 // ---------------------------------------------------------------------------------------
-// Pass B: x transforms of whole rows, with the advective product in between.
+// Pass A: inverse transforms along y of kx columns.
+// ---------------------------------------------------------------------------------------
+enum YInvSet : int { YI_STATE = 0, YI_RHS = 1, YI_VG = 2 };
+
+template <typename T, typename TIN, int NY, int SET> struct YInv2D {
+    static constexpr int F = SET == YI_STATE ? 2 : SET == YI_RHS ? 4 : 3;   // fields produced
+    static constexpr int F0 = SET == YI_VG ? 4 : 0;                          // offset in MA
+    static constexpr int UG = 2;                                             // units per sub-pass
+    static constexpr int NG = (F + UG - 1) / UG;
+    static constexpr int EPT = ept_fit<NY, EptOf<T>::v>();
+    using FFT = RegFFT<T, NY, EPT, UG, true>;
+    static constexpr int G = groups_per_block<FFT::NTR>();
+    static constexpr int NT = G * FFT::NTR;
+    static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<TIN>);   // one staged group
+    static constexpr size_t SMEM = STAGE + (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+};
+
+template <typename T, typename TIN, int NY, int SET>
+__global__ void __launch_bounds__(YInv2D<T, TIN, NY, SET>::NT)
+k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Geo g,
+         const cplx<T>* __restrict__ tw) {
+    using P = YInv2D<T, TIN, NY, SET>;
+    using FFT = typename P::FFT;
+    constexpr int EPT = P::EPT, UG = P::UG, F = P::F, G = P::G;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<TIN>* stg = reinterpret_cast<cplx<TIN>*>(smraw);
+    const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
+    const int K = g.K, KY = g.KY;
+    const int nitems = (K + G - 1) / G;
+    const int colbytes = KY * 2 * (int)sizeof(cplx<TIN>);
+    auto issue = [&](int item) {
+        const int kx0 = item * G;
+        const int ncol = min(G, K - kx0);
+        stage_line(stg, S + (size_t)kx0 * KY * 2, ncol * colbytes);
+        cp_async_commit();
+    };
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const cplx<TIN>* col = stg + (size_t)gi * KY * 2;
+        const int kx = item * G + gi;
+        const bool valid = kx < K;
+        const T kxt = (T)kx;
+        // the column's two components, in the register order of the first transform stage
+        cplx<T> ra[EPT], rb[EPT];
+#pragma unroll
+        for (int e = 0; e < EPT; ++e) {
+            const int kyi = pos_trunc(FFT::in_pos(t, e), K, KY, NY);
+            const bool on = valid && kyi >= 0;
+            ra[e] = on ? cvt<cplx<TIN>, cplx<T>>(col[2 * kyi]) : mk<T>(0, 0);
+            rb[e] = on ? cvt<cplx<TIN>, cplx<T>>(col[2 * kyi + 1]) : mk<T>(0, 0);
+        }
+        __syncthreads();   // the staging buffer is free: fetch the next column group now
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+#pragma unroll
+        for (int grp = 0; grp < P::NG; ++grp) {
+            cplx<T> v[UG * EPT];
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+                const int kyi = pos_trunc(FFT::in_pos(t, e), K, KY, NY);
+                const T ky = (T)(kyi >= 0 ? trunc_k(kyi, K, KY) : 0);
+                const cplx<T> a = ra[e], b = rb[e];
+                cplx<T> f[4];
+                if constexpr (SET == YI_STATE) {
+                    f[0] = a; f[1] = b; f[2] = f[3] = mk<T>(0, 0);
+                } else if constexpr (SET == YI_RHS) {
+                    f[0] = a; f[1] = cscale<T>(cmuli<T>(a), ky);
+                    f[2] = b; f[3] = cscale<T>(cmuli<T>(b), ky);
+                } else {
+                    const T ky2 = ky * ky;
+                    f[0] = cscale<T>(a, ky2);
+                    f[1] = cscale<T>(b, ky2);
+                    // lap(theta)^ = -i |k|^2 (kx u1^ + ky u2^)   (solution.F90:1131)
+                    const T kk = kxt * kxt + ky2;
+                    f[2] = cscale<T>(cmulni<T>(cadd<T>(cscale<T>(a, kxt), cscale<T>(b, ky))), kk);
+                    f[3] = mk<T>(0, 0);
+                }
+#pragma unroll
+                for (int u = 0; u < UG; ++u) v[u * EPT + e] = f[grp * UG + u];
+            }
+            FFT::run(v, sm, tw, t);
+            if (valid) {
+#pragma unroll
+                for (int e = 0; e < EPT; ++e) {
+                    const int y = FFT::out_pos(t, e);
+                    cplx<T>* dst = MA + ((size_t)y * K + kx) * ftot + P::F0 + grp * UG;
+                    if (grp * UG + 1 < F) st2<T>(dst, v[e], v[EPT + e]);
+                    else dst[0] = v[e];
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------------------
+// Pass B: x transforms of whole rows, with the advective product in registers.
 // ---------------------------------------------------------------------------------------
 enum XMode : int { XM_RHS = 1, XM_RHS_VG = 2, XM_TO_PHYS = 3, XM_FROM_PHYS = 4 };
 
 template <typename T, int NX, int MODE> struct XPass2D {
     static constexpr int ZU = MODE == XM_RHS ? 3 : MODE == XM_RHS_VG ? 5 : 1;   // units per row
-    static constexpr int BR = (sizeof(T) == 8 ? 1 : 2) * (ZU == 1 ? 2 : 1);      // rows per block
-    static constexpr int U = ZU * BR;
-    static constexpr int US = padded_len(NX);
-    static constexpr int NT = pick_threads<T, U * NX>();
-    static constexpr size_t SMEM_FFT = (size_t)U * US * sizeof(cplx<T>);
-    static constexpr size_t SMEM = SMEM_FFT > (size_t)9 * NT * 8 ? SMEM_FFT : (size_t)9 * NT * 8;
+    static constexpr int FIN = MODE == XM_RHS ? 4 : MODE == XM_RHS_VG ? 8 : MODE == XM_TO_PHYS ? 2 : 0;
+    static constexpr int EPT = ept_fit<NX, EptOf<T>::v>();
+    // at most three units share one shared-memory exchange; more run as a second transform
+    static constexpr int ZA = ZU > 3 ? 3 : ZU, ZB = ZU - ZA;
+    using IFFT = RegFFT<T, NX, EPT, ZA, true>;
+    using IFFTB = RegFFT<T, NX, EPT, (ZB > 0 ? ZB : 1), true>;
+    using FFFT = RegFFT<T, NX, EPT, 1, false>;
+    static constexpr int NTR = IFFT::NTR;
+    static constexpr int G = groups_per_block<NTR>();
+    static constexpr int NT = G * NTR;
+    static constexpr int KMAX = NX / 3;
+    // one staged group: G rows of K*FIN mixed values, or G rows of 2 physical components
+    static constexpr size_t STAGE = MODE == XM_FROM_PHYS ? (size_t)G * 2 * NX * sizeof(double)
+                                                          : (size_t)G * KMAX * FIN * sizeof(cplx<T>);
+    static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
+    static constexpr size_t SMEM = STAGE + XCHR;
 };
 
-// Packs two half spectra A, B (kx in [0,K)) into one length-NX complex sequence whose inverse
-// transform is a + i b, a and b the real fields.  The imaginary parts of the kx=0 bins are
-// dropped, as the reference's dreal() does.
+// Packs the half-spectrum values A, B of wavenumber k (0 <= k < K) for one position of a
+// length-NX sequence whose inverse transform is a + i b.  `mirror` selects the position NX-k
+// (conjugate side); the imaginary parts of the kx = 0 bin are dropped as dreal() does.
 template <typename T>
-__device__ __forceinline__ void pack2(cplx<T>* unit, int k, int NX, cplx<T> A, cplx<T> B) {
-    if (k == 0) {
-        unit[pidx(0)] = mk<T>(A.x, B.x);
-    } else {
-        unit[pidx(k)] = mk<T>(A.x - B.y, A.y + B.x);
-        unit[pidx(NX - k)] = mk<T>(A.x + B.y, B.x - A.y);
-    }
+__device__ __forceinline__ cplx<T> pack_at(cplx<T> A, cplx<T> B, bool mirror, bool zero_bin) {
+    if (zero_bin) return mk<T>(A.x, B.x);
+    return mirror ? mk<T>(A.x + B.y, B.x - A.y) : mk<T>(A.x - B.y, A.y + B.x);
 }
 
 template <typename T, int NX, int MODE>
@@ -117,119 +180,147 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
           const double* __restrict__ phys_in, double* __restrict__ phys_out,
           double* __restrict__ vg_part, Geo g, const cplx<T>* __restrict__ tw) {
     using P = XPass2D<T, NX, MODE>;
-    constexpr int ZU = P::ZU, BR = P::BR, US = P::US, NT = P::NT;
+    using IFFT = typename P::IFFT;
+    using FFFT = typename P::FFFT;
+    constexpr int ZU = P::ZU, EPT = P::EPT, NT = P::NT, NTR = P::NTR, G = P::G, FIN = P::FIN;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    unsigned char* stg = smraw;
+    const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * IFFT::SMEM_ELEMS;
     const int K = g.K, NY = g.ny;
-    const int y0 = blockIdx.x * BR;
-    const int tid = threadIdx.x;
+    const int nitems = (NY + G - 1) / G;
+    auto issue = [&](int item) {
+        const int y0 = item * G;
+        const int nrow = min(G, NY - y0);
+        if constexpr (MODE == XM_FROM_PHYS) {
+            double* d = reinterpret_cast<double*>(stg);
+            stage_line(d, phys_in + (size_t)y0 * NX, nrow * NX * 8);
+            stage_line(d + G * NX, phys_in + (size_t)NY * NX + (size_t)y0 * NX, nrow * NX * 8);
+        } else {
+            stage_line(stg, MA + (size_t)y0 * K * ftot, nrow * K * ftot * (int)sizeof(cplx<T>));
+        }
+        cp_async_commit();
+    };
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    double etamin = 1.0 / 0.0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const int y = item * G + gi;
+        const bool valid = y < NY;
+        cplx<T> v[ZU * EPT];
+        if constexpr (MODE == XM_FROM_PHYS) {
+            const double* row = reinterpret_cast<const double*>(stg) + (size_t)gi * NX;
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+                const int x = FFFT::in_pos(t, e);
+                v[e] = valid ? mk<T>((T)row[x], (T)row[G * NX + x]) : mk<T>(0, 0);
+            }
+        } else {
+            const cplx<T>* row = reinterpret_cast<const cplx<T>*>(stg) + (size_t)gi * K * FIN;
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+                const int p = IFFT::in_pos(t, e);
+                const bool lo = p < K, hi = p > NX - K;
+                const int k = lo ? p : NX - p;
+#pragma unroll
+                for (int u = 0; u < ZU; ++u) v[u * EPT + e] = mk<T>(0, 0);
+                if (valid && (lo || hi)) {
+                    const cplx<T>* src = row + (size_t)k * FIN;
+                    const bool z0 = p == 0;
+                    const cplx<T> g1 = src[0];
+                    if constexpr (MODE == XM_TO_PHYS) {
+                        v[e] = pack_at<T>(g1, src[1], hi, z0);
+                    } else {
+                        const cplx<T> h1 = src[1], g2 = src[2], h2 = src[3];
+                        const T kx = (T)k;
+                        v[e] = pack_at<T>(g1, g2, hi, z0);
+                        v[EPT + e] = pack_at<T>(cscale<T>(cmuli<T>(g1), kx), cscale<T>(cmuli<T>(g2), kx), hi, z0);
+                        v[2 * EPT + e] = pack_at<T>(h1, h2, hi, z0);
+                        if constexpr (MODE == XM_RHS_VG) {
+                            const cplx<T> q1 = src[4], q2 = src[5], th = src[6];
+                            const T kx2 = kx * kx;
+                            v[3 * EPT + e] = pack_at<T>(csub<T>(cscale<T>(g1, -kx2), q1),
+                                                        csub<T>(cscale<T>(g2, -kx2), q2), hi, z0);
+                            v[4 * EPT + e] = pack_at<T>(th, mk<T>(0, 0), hi, z0);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();   // the staging buffer is free: fetch the next row group now
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        if constexpr (MODE != XM_FROM_PHYS) {
+            IFFT::run(v, sm, tw, t);
+            if constexpr (P::ZB > 0) P::IFFTB::run(v + P::ZA * EPT, sm, tw, t);
+        }
 
-    if constexpr (MODE == XM_FROM_PHYS) {
-        for (int e = tid; e < BR * NX; e += NT) {
-            const int r = e / NX, x = e - r * NX;
-            const size_t o = (size_t)(y0 + r) * NX + x;
-            sm[r * US + pidx(x)] = mk<T>((T)phys_in[o], (T)phys_in[(size_t)NY * NX + o]);
-        }
-    } else {
-        // zero the untouched middle band of every unit
-        for (int e = tid; e < BR * ZU * (NX - 2 * K + 1); e += NT) {
-            const int u = e / (NX - 2 * K + 1), x = K + (e - u * (NX - 2 * K + 1));
-            sm[u * US + pidx(x)] = mk<T>(0, 0);
-        }
-        for (int e = tid; e < BR * K; e += NT) {
-            const int r = e / K, k = e - r * K;
-            const cplx<T>* src = MA + ((size_t)(y0 + r) * K + k) * ftot;
-            cplx<T>* z = sm + r * ZU * US;
-            const cplx<T> g1 = src[0];
-            if constexpr (MODE == XM_TO_PHYS) {
-                pack2<T>(z, k, NX, g1, src[1]);
-            } else {
-                const cplx<T> h1 = src[1], g2 = src[2], h2 = src[3];
-                const T kx = (T)k;
-                pack2<T>(z, k, NX, g1, g2);
-                pack2<T>(z + US, k, NX, cscale<T>(cmuli<T>(g1), kx), cscale<T>(cmuli<T>(g2), kx));
-                pack2<T>(z + 2 * US, k, NX, h1, h2);
-                if constexpr (MODE == XM_RHS_VG) {
-                    const cplx<T> q1 = src[4], q2 = src[5], t = src[6];
-                    const T kx2 = kx * kx;
-                    cplx<T> l1 = csub<T>(cscale<T>(g1, -kx2), q1);
-                    cplx<T> l2 = csub<T>(cscale<T>(g2, -kx2), q2);
-                    pack2<T>(z + 3 * US, k, NX, l1, l2);
-                    pack2<T>(z + 4 * US, k, NX, t, mk<T>(0, 0));
+        if constexpr (MODE == XM_TO_PHYS) {
+            if (valid) {
+#pragma unroll
+                for (int e = 0; e < EPT; ++e) {
+                    const int x = IFFT::out_pos(t, e);
+                    const size_t o = (size_t)y * NX + x;
+                    phys_out[o] = (double)v[e].x;
+                    phys_out[(size_t)NY * NX + o] = (double)v[e].y;
+                }
+            }
+        } else {
+            if constexpr (MODE == XM_RHS || MODE == XM_RHS_VG) {
+                // advective product (solution.F90:841-846) at the points this thread holds; the
+                // viscous term is added spectrally in pass C
+                const double nu = g.nu;
+#pragma unroll
+                for (int e = 0; e < EPT; ++e) {
+                    const cplx<T> a = v[e], b = v[EPT + e], c = v[2 * EPT + e];
+                    const T u1 = a.x, u2 = a.y, u1x = b.x, u2x = b.y, u1y = c.x, u2y = c.y;
+                    const T n1 = -u1 * u1x - u2 * u1y;
+                    const T n2 = -u1 * u2x - u2 * u2y;
+                    v[e] = mk<T>(n1, n2);
+                    if constexpr (MODE == XM_RHS_VG) {
+                        if (valid) {
+                            // velgrad_calculate2D (solution.F90:1149-1166), accumulated in FP64
+                            const cplx<T> l = v[3 * EPT + e], th = v[4 * EPT + e];
+                            const double U1 = u1, U2 = u2, D11 = u1x, D22 = u2y, D12 = u1y, D21 = u2x;
+                            const double div = D11 + D22;
+                            const double uu = U1 * U1 + U2 * U2;
+                            acc[0] += div * div * uu;
+                            acc[1] += (D11 * D11 + D22 * D22 + 2.0 * D12 * D21) * uu;
+                            acc[2] += div * uu;
+                            acc[3] += 2.0 * U1 * div * (double)l.x + 2.0 * U2 * div * (double)l.y + uu * (double)th.x;
+                            acc[4] += nu * (D12 - D21) * (D12 - D21) + nu * div * div;
+                            etamin = fmin(etamin, sqrt(nu / fabs(div)));
+                            acc[5] += uu;
+                            acc[6] += D11 * D11 + D22 * D22;
+                        }
+                    }
+                }
+            }
+            // forward transform of the packed product (or of the packed physical fields)
+            FFFT::run(v, sm, tw, t);
+            // split the packed spectrum into the two half spectra, kx in [0,K): Z[k] and Z[NX-k]
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) sm[pidx(FFFT::out_pos(t, e))] = v[e];
+            __syncthreads();
+            if (valid) {
+                for (int k = t; k < K; k += NTR) {
+                    const cplx<T> Z = sm[pidx(k)];
+                    const cplx<T> Zc = cconj<T>(sm[pidx(k == 0 ? 0 : NX - k)]);
+                    st2<T>(MB + ((size_t)k * NY + y) * 2, cscale<T>(cadd<T>(Z, Zc), (T)0.5),
+                           cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5));
                 }
             }
         }
     }
-    __syncthreads();
-
-    if constexpr (MODE == XM_FROM_PHYS) {
-        fft_run<T, NX, BR, US, NT, false>(sm, tw);
-    } else {
-        fft_run<T, NX, BR * ZU, US, NT, true>(sm, tw);
-    }
-
-    if constexpr (MODE == XM_TO_PHYS) {
-        for (int e = tid; e < BR * NX; e += NT) {
-            const int r = e / NX, x = e - r * NX;
-            const cplx<T> z = sm[r * US + pidx(x)];
-            const size_t o = (size_t)(y0 + r) * NX + x;
-            phys_out[o] = (double)z.x;
-            phys_out[(size_t)NY * NX + o] = (double)z.y;
-        }
-        return;
-    }
-
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    double etamin = 1.0 / 0.0;
-    if constexpr (MODE == XM_RHS || MODE == XM_RHS_VG) {
-        // advective product (solution.F90:841-846); the viscous term is added spectrally in pass C
-        const double nu = g.nu;
-        for (int e = tid; e < BR * NX; e += NT) {
-            const int r = e / NX, x = e - r * NX;
-            cplx<T>* z = sm + r * ZU * US;
-            const cplx<T> a = z[pidx(x)], b = z[US + pidx(x)], c = z[2 * US + pidx(x)];
-            const T u1 = a.x, u2 = a.y, u1x = b.x, u2x = b.y, u1y = c.x, u2y = c.y;
-            const T n1 = -u1 * u1x - u2 * u1y;
-            const T n2 = -u1 * u2x - u2 * u2y;
-            z[pidx(x)] = mk<T>(n1, n2);
-            if constexpr (MODE == XM_RHS_VG) {
-                // velgrad_calculate2D (solution.F90:1149-1166), accumulated in FP64
-                const cplx<T> l = z[3 * US + pidx(x)], th = z[4 * US + pidx(x)];
-                const double U1 = u1, U2 = u2, D11 = u1x, D22 = u2y, D12 = u1y, D21 = u2x;
-                const double div = D11 + D22;
-                const double uu = U1 * U1 + U2 * U2;
-                acc[0] += div * div * uu;
-                acc[1] += (D11 * D11 + D22 * D22 + 2.0 * D12 * D21) * uu;
-                acc[2] += div * uu;
-                acc[3] += 2.0 * U1 * div * (double)l.x + 2.0 * U2 * div * (double)l.y + uu * (double)th.x;
-                acc[4] += nu * (D12 - D21) * (D12 - D21) + nu * div * div;
-                etamin = fmin(etamin, sqrt(nu / fabs(div)));
-                acc[5] += uu;
-                acc[6] += D11 * D11 + D22 * D22;
-            }
-        }
-        __syncthreads();
-        fft_run<T, NX, BR, US, NT, false, 1, ZU * US>(sm, tw);
-    }
-
-    // split the packed forward transform into the two half spectra, kx in [0,K)
-    for (int e = tid; e < BR * K; e += NT) {
-        const int r = e / K, k = e - r * K;
-        const cplx<T>* z = sm + r * ZU * US;
-        const cplx<T> Z = z[pidx(k)];
-        const cplx<T> Zc = cconj<T>(z[pidx(k == 0 ? 0 : NX - k)]);
-        const cplx<T> A = cscale<T>(cadd<T>(Z, Zc), (T)0.5);
-        const cplx<T> B = cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5);
-        cplx<T>* dst = MB + ((size_t)k * NY + y0 + r) * 2;
-        dst[0] = A;
-        dst[1] = B;
-    }
+    cp_async_wait<0>();
     if constexpr (MODE == XM_RHS_VG) {
         __syncthreads();
-        double* scratch = reinterpret_cast<double*>(smraw);
+        double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
         block_sum<7, NT>(acc, scratch);
         const double em = block_min<NT>(etamin, scratch);
-        if (tid == 0) {
+        if (threadIdx.x == 0) {
 #pragma unroll
             for (int i = 0; i < 7; ++i) vg_part[(size_t)blockIdx.x * 8 + i] = acc[i];
             vg_part[(size_t)blockIdx.x * 8 + 7] = em;
@@ -238,13 +329,17 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
 }
 
 // ---------------------------------------------------------------------------------------
-// Pass C: forward transforms along y of one kx column + spectral epilogue.
+// Pass C: forward transforms along y of kx columns + spectral epilogue.
 // ---------------------------------------------------------------------------------------
 template <typename T, int NY> struct YFwd2D {
-    static constexpr int US = padded_len(NY);
-    static constexpr int NT = pick_threads<T, 2 * NY>();
-    static constexpr size_t SMEM_FFT = (size_t)2 * US * sizeof(cplx<T>);
-    static constexpr size_t SMEM = SMEM_FFT > (size_t)NT * 8 ? SMEM_FFT : (size_t)NT * 8;
+    static constexpr int EPT = ept_fit<NY, EptOf<T>::v>();
+    using FFT = RegFFT<T, NY, EPT, 2, false>;
+    static constexpr int G = groups_per_block<FFT::NTR>();
+    static constexpr int NT = G * FFT::NTR;
+    static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<T>);
+    static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
+    static constexpr size_t SMEM = STAGE + XCHR;
 };
 
 template <typename T, int NY, int EPI>
@@ -252,47 +347,72 @@ __global__ void __launch_bounds__(YFwd2D<T, NY>::NT)
 k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
          const cplx<T>* __restrict__ tw) {
     using P = YFwd2D<T, NY>;
-    constexpr int US = P::US, NT = P::NT;
+    using FFT = typename P::FFT;
+    constexpr int EPT = P::EPT, NT = P::NT, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
-    const int kx = blockIdx.x;
+    cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
+    const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
     const int K = g.K, KY = g.KY;
-    const int tid = threadIdx.x;
-    const cplx<T>* src = MB + (size_t)kx * NY * 2;
-    for (int e = tid; e < NY * 2; e += NT) {
-        const int y = e >> 1, c = e & 1;
-        sm[c * US + pidx(y)] = src[e];
-    }
-    __syncthreads();
-    fft_run<T, NY, 2, US, NT, false>(sm, tw);
-
+    const int nitems = (K + G - 1) / G;
+    auto issue = [&](int item) {
+        const int kx0 = item * G;
+        const int ncol = min(G, K - kx0);
+        stage_line(stg, MB + (size_t)kx0 * NY * 2, ncol * NY * 2 * (int)sizeof(cplx<T>));
+        cp_async_commit();
+    };
     const double inv_n = g.inv_n;
     const long long K2 = (long long)K * K;
-    const double w = kx == 0 ? 1.0 : 2.0;
     double en = 0.0;
-    for (int kyi = tid; kyi < KY; kyi += NT) {
-        const int ky = trunc_k(kyi, K, KY);
-        const int p = trunc_pos(kyi, K, KY, NY);
-        const size_t o = ((size_t)kx * KY + kyi) * 2;
-        const long long m2i = (long long)kx * kx + (long long)ky * ky;
-        double2 v[2];
-        if (m2i < K2) {   // spherical 2/3 rule, tool.F90:185-193
-            v[0] = dscale(cvt<cplx<T>, double2>(sm[pidx(p)]), inv_n);
-            v[1] = dscale(cvt<cplx<T>, double2>(sm[US + pidx(p)]), inv_n);
-        } else {
-            v[0] = make_double2(0, 0);
-            v[1] = make_double2(0, 0);
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const cplx<T>* col = stg + (size_t)gi * NY * 2;
+        const int kx = item * G + gi;
+        const bool valid = kx < K;
+        cplx<T> v[2 * EPT];
+#pragma unroll
+        for (int e = 0; e < EPT; ++e) {
+            const int y = FFT::in_pos(t, e);
+            v[e] = valid ? col[2 * y] : mk<T>(0, 0);
+            v[EPT + e] = valid ? col[2 * y + 1] : mk<T>(0, 0);
         }
-        const double kv[2] = {(double)kx, (double)ky};
-        rk_epilogue<T, 2, EPI>(v, kv, (double)m2i, o, io, input_is_u0 != 0, g, w, en);
+        __syncthreads();   // the staging buffer is free: fetch the next column group now
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        FFT::run(v, sm, tw, t);
+        if (valid) {
+            const double w = kx == 0 ? 1.0 : 2.0;
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+                const int p = FFT::out_pos(t, e);
+                const int kyi = pos_trunc(p, K, KY, NY);
+                if (kyi < 0) continue;
+                const int ky = trunc_k(kyi, K, KY);
+                const size_t o = ((size_t)kx * KY + kyi) * 2;
+                const long long m2i = (long long)kx * kx + (long long)ky * ky;
+                double2 vv[2];
+                if (m2i < K2) {   // spherical 2/3 rule, tool.F90:185-193
+                    vv[0] = dscale(cvt<cplx<T>, double2>(v[e]), inv_n);
+                    vv[1] = dscale(cvt<cplx<T>, double2>(v[EPT + e]), inv_n);
+                } else {
+                    vv[0] = make_double2(0, 0);
+                    vv[1] = make_double2(0, 0);
+                }
+                const double kv[2] = {(double)kx, (double)ky};
+                rk_epilogue<T, 2, EPI>(vv, kv, (double)m2i, o, io, input_is_u0 != 0, g, w, en);
+            }
+        }
     }
+    cp_async_wait<0>();
     if constexpr (EPI == EPI_RK3 || EPI == EPI_CN_LAST) {
         if (io.energy_part) {
             __syncthreads();
-            double* scratch = reinterpret_cast<double*>(smraw);
-            double v[1] = {en};
-            block_sum<1, NT>(v, scratch);
-            if (tid == 0) io.energy_part[kx] = v[0];
+            double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
+            double r[1] = {en};
+            block_sum<1, NT>(r, scratch);
+            if (threadIdx.x == 0) io.energy_part[blockIdx.x] = r[0];
         }
     }
 }

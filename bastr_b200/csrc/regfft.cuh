@@ -1,0 +1,143 @@
+// Register-resident Stockham FFT for sm_100a.
+//
+// A group of NTR = N/EPT threads transforms UPT units (independent length-N complex sequences
+// that share one index map) of which every thread holds EPT elements per unit in registers.
+// Stage s of radix R works on butterflies b = t + q*NTR (q < EPT/R) reading x[b + j*N/R]:
+// twiddle, DFT-R in registers, and the outputs land at (b-k)*R + k + j*P (k = b mod P, P the
+// product of the earlier radices), the Stockham autosort order.  Only the hand-over between two
+// stages goes through shared memory; the first stage takes its inputs from the caller's
+// registers (filled straight from global memory by `in_pos`) and the last stage leaves its
+// outputs in registers at `out_pos`, so a pass needs no shared-memory copy of its input or
+// output.  The inverse plan uses radix EPT first and the remainder last; the forward plan is
+// its mirror, so an inverse transform followed by a forward one of the same shape hands its
+// registers over directly (out_pos of the first == in_pos of the second).
+//
+// Twiddles w^m = exp(-2 pi i m/N) come from a table generated on the host in extended
+// precision and rounded once to T; per butterfly only w^1, w^2, w^4, w^8 are loaded and the
+// other powers are formed by at most two multiplications, and they are shared by all units.
+#pragma once
+#include "fft_engine.cuh"
+
+namespace bastr {
+
+__host__ __device__ constexpr int ilog2c(int n) {
+    int r = 0;
+    while ((1 << r) < n) ++r;
+    return r;
+}
+
+template <int N, int EPT> struct RPlan {
+    static constexpr int n = ilog2c(N), e = ilog2c(EPT);
+    static constexpr int NFULL = n / e, REM = n % e;
+    static constexpr int NS = NFULL + (REM ? 1 : 0);
+    static constexpr int inv_radix(int s) { return s < NFULL ? EPT : (1 << REM); }
+    static constexpr int fwd_radix(int s) { return inv_radix(NS - 1 - s); }
+    static constexpr int radix(bool inv, int s) { return inv ? inv_radix(s) : fwd_radix(s); }
+    // product of the radices before stage s
+    static constexpr int sub(bool inv, int s) { return s == 0 ? 1 : sub(inv, s - 1) * radix(inv, s - 1); }
+};
+
+template <typename T, int N, int EPT, int UPT, bool INV>
+struct RegFFT {
+    using PL = RPlan<N, EPT>;
+    static constexpr int NTR = N / EPT;
+    static constexpr int NS = PL::NS;
+    static constexpr int R0 = PL::radix(INV, 0);
+    static constexpr int RL = PL::radix(INV, NS - 1);
+    static constexpr int US = padded_len(N);                // shared elements per unit
+    static constexpr int SMEM_ELEMS = UPT * US;
+    static_assert((N & (N - 1)) == 0 && N >= EPT, "power-of-two length");
+
+    // position of register element e of thread t before the first stage / after the last
+    __device__ static __forceinline__ int in_pos(int t, int e) {
+        return t + (e / R0) * NTR + (e % R0) * (N / R0);
+    }
+    __device__ static __forceinline__ int out_pos(int t, int e) {
+        return t + (e / RL) * NTR + (e % RL) * (N / RL);
+    }
+
+    template <int R, int PS>
+    __device__ static __forceinline__ void compute(cplx<T>* v, const cplx<T>* __restrict__ tw, int t) {
+#pragma unroll
+        for (int q = 0; q < EPT / R; ++q) {
+            const int b = t + q * NTR;
+            if constexpr (PS > 1) {
+                constexpr int S = N / (PS * R);
+                const int k = b & (PS - 1);
+                cplx<T> w[R];
+                w[1] = tw[k * S];
+                if constexpr (R >= 4) {
+                    w[2] = tw[2 * k * S];
+                    w[3] = cmul<T>(w[2], w[1]);
+                }
+                if constexpr (R >= 8) {
+                    w[4] = tw[4 * k * S];
+                    w[5] = cmul<T>(w[4], w[1]);
+                    w[6] = cmul<T>(w[4], w[2]);
+                    w[7] = cmul<T>(w[4], w[3]);
+                }
+                if constexpr (R >= 16) {
+                    w[8] = tw[8 * k * S];
+#pragma unroll
+                    for (int j = 9; j < 16; ++j) w[j] = cmul<T>(w[8], w[j - 8]);
+                }
+#pragma unroll
+                for (int j = 1; j < R; ++j) {
+                    const cplx<T> ww = INV ? cconj<T>(w[j]) : w[j];
+#pragma unroll
+                    for (int u = 0; u < UPT; ++u) v[u * EPT + q * R + j] = cmul<T>(v[u * EPT + q * R + j], ww);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UPT; ++u) dftR<T, INV, R>(v + u * EPT + q * R);
+        }
+    }
+
+    template <int R, int PS, int R2>
+    __device__ static __forceinline__ void exchange(cplx<T>* v, cplx<T>* sm, int t) {
+#pragma unroll
+        for (int q = 0; q < EPT / R; ++q) {
+            const int b = t + q * NTR;
+            const int k = b & (PS - 1);
+            const int base = (b - k) * R + k;
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+#pragma unroll
+                for (int u = 0; u < UPT; ++u) sm[u * US + pidx(base + j * PS)] = v[u * EPT + q * R + j];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < EPT / R2; ++q) {
+#pragma unroll
+            for (int j = 0; j < R2; ++j) {
+                const int p = t + q * NTR + j * (N / R2);
+#pragma unroll
+                for (int u = 0; u < UPT; ++u) v[u * EPT + q * R2 + j] = sm[u * US + pidx(p)];
+            }
+        }
+        __syncthreads();
+    }
+
+    template <int S>
+    __device__ static __forceinline__ void stages(cplx<T>* v, cplx<T>* sm, const cplx<T>* __restrict__ tw, int t) {
+        if constexpr (S < NS) {
+            constexpr int R = PL::radix(INV, S);
+            constexpr int PS = PL::sub(INV, S);
+            compute<R, PS>(v, tw, t);
+            if constexpr (S + 1 < NS) {
+                exchange<R, PS, PL::radix(INV, S + 1)>(v, sm, t);
+            }
+            stages<S + 1>(v, sm, tw, t);
+        }
+    }
+
+    // v: UPT*EPT registers (unit-major); sm: this group's SMEM_ELEMS shared elements.
+    // The caller fills v in in_pos order; on return v holds the transform in out_pos order.
+    // Contains __syncthreads(): every thread of the block must call it.
+    __device__ static __forceinline__ void run(cplx<T>* v, cplx<T>* sm, const cplx<T>* __restrict__ tw, int t) {
+        stages<0>(v, sm, tw, t);
+    }
+};
+
+}  // namespace bastr

@@ -187,6 +187,26 @@ __device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double 
     }
 }
 
+// Asynchronous 16-byte global -> shared copies (cp.async, bypassing L1), used to stage whole
+// contiguous lines one iteration ahead of the transform that consumes them.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPEND> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+}
+
+// Copies `bytes` (a multiple of 16, both ends 16-byte aligned) from global to shared memory with
+// all threads of the block; returns without waiting.
+__device__ __forceinline__ void stage_line(void* smem_dst, const void* gmem_src, int bytes) {
+    const int n16 = bytes >> 4;
+    char* d = static_cast<char*>(smem_dst);
+    const char* s = static_cast<const char*>(gmem_src);
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(d + 16 * i, s + 16 * i);
+}
+
 // Lines (or rows) per block so that one block holds about 48 KB of transform data; a power of 2.
 template <typename T> __host__ __device__ constexpr int target_elems() { return sizeof(T) == 8 ? 3072 : 6144; }
 template <typename T, int N, int F> __host__ __device__ constexpr int lines_per_block() {

@@ -280,7 +280,7 @@ def ours(args):
     device = dist_ctx.local if dist_ctx else 0
     torch.cuda.set_device(device)
     peak, peak_kind = hbm_peak()
-    wl, prec = HEADLINE
+    wl, prec = args.workload, args.precision
     w = WORKLOADS[wl]
     sampler = ClockSampler(device) if rank == 0 else None
     s, u, stream, ms, clocks, info = measure(wl, prec, args.steps, args.warmup, device, dist_ctx, sampler)
@@ -316,9 +316,11 @@ def ours(args):
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": n_gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if prec == "fp32" else "f64",
         "data": "synthetic (seeded Gaussian field, numpy PCG64 seed 0)",
-        "config": {"workload": w["desc"], "precision": "fp32 fields/FFTs/product, fp64 state+reductions+RK",
+        "config": {"workload": w["desc"],
+                   "precision": "fp32 fields/FFTs/product, fp64 state+reductions+RK" if prec == "fp32" else "fp64",
                    "grid": [w["ia"], w["ja"], w["ka"]],
                    "parallelism": "replicas" if n_gpus > 1 else "single GPU, whole field resident",
                    "l2": "no flush: per-step working set and traffic exceed the 126 MB L2"},
@@ -359,6 +361,9 @@ def main():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=HEADLINE[0],
+                    help="headline workload (default: the 2048^2 band-forced case)")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default=HEADLINE[1])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
