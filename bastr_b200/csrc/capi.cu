@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <set>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -147,13 +148,13 @@ template <> const cplx<float>* twp<float>(const Twiddles& t) { return t.d32; }
 // Enables the dynamic shared memory a kernel instance asks for and returns how many of its
 // blocks fit on one SM; both once per (device, kernel).
 std::mutex g_prep_mu;
-std::map<std::pair<int, const void*>, int> g_prepped;
+std::map<std::tuple<int, const void*, size_t>, int> g_prepped;
 int g_num_sms[64] = {};
 template <typename K> cudaError_t prep(K kernel, size_t smem, int nt = 0, int* blocks_per_sm = nullptr) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const auto key = std::make_pair(dev, (const void*)kernel);
+    const auto key = std::make_tuple(dev, (const void*)kernel, smem);
     std::lock_guard<std::mutex> lk(g_prep_mu);
     auto it = g_prepped.find(key);
     if (it == g_prepped.end()) {
@@ -212,13 +213,14 @@ cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
     SIZE_CASES(h->g.ny, {
         using P = YInv2D<T, TIN, NN, SET>;
         auto k = k2d_yinv<T, TIN, NN, SET>;
+        const size_t smem = P::smem(h->g.KY);
         int grid = 1;
-        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K, P::G), &grid);
+        cudaError_t e = persistent_grid(k, smem, P::NT, cdiv(h->g.K, P::G), &grid);
         if (e != cudaSuccess) return e;
         const double K_ = h->g.K;
         ProfScope ps(h, SET == YI_VG ? "k2d_yinv_vg" : "k2d_yinv",
                      K_ * h->g.KY * 2 * sizeof(cplx<TIN>) + (double)h->g.ny * K_ * P::F * sizeof(cplx<T>));
-        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[1]));
+        k<<<grid, P::NT, smem, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[1]));
     });
     return cudaGetLastError();
 }
@@ -307,15 +309,16 @@ cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
 template <typename T, typename TIN, int SET>
 cudaError_t l3_zinv(bastr_handle* h, const void* S, void* MA, int ftot) {
     SIZE_CASES3(h->g.nz, {
-        using P = ZInv3D<T, NN, SET>;
+        using P = ZInv3D<T, TIN, NN, SET>;
         auto k = k3d_zinv<T, TIN, NN, SET>;
-        cudaError_t e = prep(k, P::SMEM);
+        const size_t smem = P::smem(h->g.KZ);
+        int grid = 1;
+        cudaError_t e = persistent_grid(k, smem, P::NT, cdiv(h->g.K * h->g.KY, P::G), &grid);
         if (e != cudaSuccess) return e;
         const double lines = (double)h->g.K * h->g.KY;
         ProfScope ps(h, SET == ZI_VG ? "k3d_zinv_vg" : "k3d_zinv",
                      lines * h->g.KZ * 3 * sizeof(cplx<TIN>) + lines * h->g.nz * P::F * sizeof(cplx<T>));
-        k<<<cdiv(h->g.K * h->g.KY, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot,
-                                                                         h->g, twp<T>(h->tw[2]));
+        k<<<grid, P::NT, smem, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[2]));
     });
     return cudaGetLastError();
 }
@@ -325,13 +328,14 @@ cudaError_t l3_yinv(bastr_handle* h, const void* MA, void* MB) {
     SIZE_CASES3(h->g.ny, {
         using P = YInv3D<T, NN, SET>;
         auto k = k3d_yinv<T, NN, SET>;
-        cudaError_t e = prep(k, P::SMEM);
+        const size_t smem = P::smem(h->g.KY);
+        int grid = 1;
+        cudaError_t e = persistent_grid(k, smem, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
         if (e != cudaSuccess) return e;
         const double cs = sizeof(cplx<T>);
         ProfScope ps(h, SET == YB_RHS_VG ? "k3d_yinv_vg" : "k3d_yinv",
                      (double)h->g.K * h->g.nz * (h->g.KY * P::FIN + h->g.ny * P::F) * cs);
-        k<<<cdiv(h->g.K * h->g.nz, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, (cplx<T>*)MB, h->g,
-                                                                         twp<T>(h->tw[1]));
+        k<<<grid, P::NT, smem, h->stream>>>((const cplx<T>*)MA, (cplx<T>*)MB, h->g, twp<T>(h->tw[1]));
     });
     return cudaGetLastError();
 }
@@ -341,15 +345,17 @@ cudaError_t l3_xpass(bastr_handle* h, const void* MB, void* MC, const double* pi
     SIZE_CASES3(h->g.nx, {
         using P = XPass3D<T, NN, MODE>;
         auto k = k3d_xpass<T, NN, MODE>;
-        cudaError_t e = prep(k, P::SMEM);
+        int grid = 1;
+        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.ny * h->g.nz, P::G), &grid);
         if (e != cudaSuccess) return e;
+        if (MODE == X3_RHS_VG) h->n_vg_blocks = grid;
         const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.nz * h->g.K;
         const double phys = 3.0 * h->g.nx * h->g.ny * h->g.nz * 8;
         const double b = MODE == X3_RHS ? mix * 12 * cs : MODE == X3_RHS_VG ? mix * 16 * cs
                        : MODE == X3_TO_PHYS ? mix * 3 * cs + phys : phys + mix * 3 * cs;
         ProfScope ps(h, MODE == X3_RHS_VG ? "k3d_xpass_vg" : MODE == X3_RHS ? "k3d_xpass" : "k3d_xpass_state", b);
-        k<<<cdiv(h->g.ny * h->g.nz, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg,
-                                                                       h->g, twp<T>(h->tw[0]));
+        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg, h->g,
+                                                twp<T>(h->tw[0]));
     });
     return cudaGetLastError();
 }
@@ -359,11 +365,11 @@ cudaError_t l3_yfwd(bastr_handle* h, const void* MC, void* MD) {
     SIZE_CASES3(h->g.ny, {
         using P = YFwd3D<T, NN>;
         auto k = k3d_yfwd<T, NN>;
-        cudaError_t e = prep(k, P::SMEM);
+        int grid = 1;
+        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
         if (e != cudaSuccess) return e;
         ProfScope ps(h, "k3d_yfwd", (double)h->g.K * h->g.nz * (h->g.ny + h->g.KY) * 3 * sizeof(cplx<T>));
-        k<<<cdiv(h->g.K * h->g.nz, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MC, (cplx<T>*)MD, h->g,
-                                                                         twp<T>(h->tw[1]));
+        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MC, (cplx<T>*)MD, h->g, twp<T>(h->tw[1]));
     });
     return cudaGetLastError();
 }
@@ -373,44 +379,15 @@ cudaError_t l3_zfwd(bastr_handle* h, const void* MD, StageIO<T> io, int from_u0)
     SIZE_CASES3(h->g.nz, {
         using P = ZFwd3D<T, NN>;
         auto k = k3d_zfwd<T, NN, EPI>;
-        cudaError_t e = prep(k, P::SMEM);
+        int grid = 1;
+        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K * h->g.KY, P::G), &grid);
         if (e != cudaSuccess) return e;
+        if (io.energy_part) h->n_en_blocks = grid;
         const double cs = sizeof(cplx<T>), lines = (double)h->g.K * h->g.KY;
         ProfScope ps(h, "k3d_zfwd", lines * h->g.nz * 3 * cs + epi_bytes(EPI, from_u0, lines * h->g.KZ * 3, cs));
-        k<<<cdiv(h->g.K * h->g.KY, P::G), P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MD, io, from_u0, h->g,
-                                                                         twp<T>(h->tw[2]));
+        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MD, io, from_u0, h->g, twp<T>(h->tw[2]));
     });
     return cudaGetLastError();
-}
-
-template <typename T> int zfwd_lines(int nz) {
-    switch (nz) {
-        case 16: return ZFwd3D<T, 16>::G;
-        case 32: return ZFwd3D<T, 32>::G;
-        case 64: return ZFwd3D<T, 64>::G;
-        case 128: return ZFwd3D<T, 128>::G;
-        case 256: return ZFwd3D<T, 256>::G;
-        default: return ZFwd3D<T, 512>::G;
-    }
-}
-template <typename T> int xpass3_rows_vg(int nx) {
-    switch (nx) {
-        case 16: return XPass3D<T, 16, X3_RHS_VG>::G;
-        case 32: return XPass3D<T, 32, X3_RHS_VG>::G;
-        case 64: return XPass3D<T, 64, X3_RHS_VG>::G;
-        case 128: return XPass3D<T, 128, X3_RHS_VG>::G;
-        case 256: return XPass3D<T, 256, X3_RHS_VG>::G;
-        default: return XPass3D<T, 512, X3_RHS_VG>::G;
-    }
-}
-
-int vg_blocks3d(bastr_handle* h) {
-    const int br = h->fp32 ? xpass3_rows_vg<float>(h->g.nx) : xpass3_rows_vg<double>(h->g.nx);
-    return cdiv(h->g.ny * h->g.nz, br);
-}
-int en_blocks3d(bastr_handle* h) {
-    const int l = h->fp32 ? zfwd_lines<float>(h->g.nz) : zfwd_lines<double>(h->g.nz);
-    return cdiv(h->g.K * h->g.KY, l);
 }
 
 // Mixed-field buffer sizes (bytes) for compute element size cs.
@@ -740,8 +717,8 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
         dev_alloc(h, &h->ma, ma, st);
         dev_alloc(h, &h->mb, mb, st);
         dev_alloc(h, &h->mc, mc, st);
-        h->n_vg_blocks = vg_blocks3d(h);
-        h->n_en_blocks = en_blocks3d(h);
+        h->n_vg_blocks = 1;   // set by the launches (persistent grids)
+        h->n_en_blocks = 1;
     }
     dev_alloc(h, &h->u0, h->n_state * sizeof(double2), st);
     dev_alloc(h, &h->us, h->n_state * cs, st);

@@ -247,14 +247,14 @@ __global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__
                                                       Geo g, double* __restrict__ rec) {
     __shared__ double scratch[7 * NT];
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    double em = 1.0 / 0.0;
+    double dm = 0.0;   // largest |theta| over the grid
     for (int b = threadIdx.x; b < nblk; b += NT) {
 #pragma unroll
         for (int i = 0; i < 7; ++i) acc[i] += part[(size_t)b * 8 + i];
-        em = fmin(em, part[(size_t)b * 8 + 7]);
+        dm = fmax(dm, part[(size_t)b * 8 + 7]);
     }
     block_sum<7, NT>(acc, scratch);
-    em = block_min<NT>(em, scratch);
+    dm = -block_min<NT>(-dm, scratch);
     if (threadIdx.x == 0) {
         const double N = (double)g.nx * (double)g.ny * (double)g.nz;
         const double nu = g.nu;
@@ -264,9 +264,10 @@ __global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__
         const double u2theta = acc[2] / N;
         const double dissp = acc[3] / N;
         const double epsilon = acc[4] / N;
-        // eta_min starts at the default-real product 2*3.14 (solution.F90:1145, 1236)
+        // eta_min starts at the default-real product 2*3.14 (solution.F90:1145, 1236); the
+        // minimum of sqrt(nu/|theta|) over the points is sqrt(nu/max|theta|)
         const double eta0 = (double)(2.0f * 3.14f);
-        const double eta_min = fmin(eta0, em);
+        const double eta_min = fmin(eta0, sqrt(nu / dm));
         const double urms = sqrt(acc[5] / N);
         const double dudx2 = acc[6] / N;
         const double ufluc = urms / sqrt(dd);

@@ -24,9 +24,39 @@ template <> struct cvec<double> { using t = double2; };
 template <typename T> using cplx = typename cvec<T>::t;
 
 template <typename T> __device__ __forceinline__ cplx<T> mk(T x, T y) { cplx<T> r; r.x = x; r.y = y; return r; }
-template <typename T> __device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
-template <typename T> __device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
-template <typename T> __device__ __forceinline__ cplx<T> cscale(cplx<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
+
+// Single-precision complex add/subtract/scale map onto Blackwell's packed FP32x2 instructions
+// (add/sub/mul.rn.f32x2): one instruction for both components.
+__device__ __forceinline__ unsigned long long f2bits(float2 a) { return *reinterpret_cast<unsigned long long*>(&a); }
+__device__ __forceinline__ float2 bitsf2(unsigned long long b) { return *reinterpret_cast<float2*>(&b); }
+__device__ __forceinline__ float2 add_f32x2(float2 a, float2 b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2bits(a)), "l"(f2bits(b)));
+    return bitsf2(r);
+}
+__device__ __forceinline__ float2 sub_f32x2(float2 a, float2 b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2bits(a)), "l"(f2bits(b)));
+    return bitsf2(r);
+}
+__device__ __forceinline__ float2 mul_f32x2(float2 a, float2 b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2bits(a)), "l"(f2bits(b)));
+    return bitsf2(r);
+}
+
+template <typename T> __device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b) {
+    if constexpr (sizeof(T) == 4) return add_f32x2(a, b);
+    else return mk<T>(a.x + b.x, a.y + b.y);
+}
+template <typename T> __device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) {
+    if constexpr (sizeof(T) == 4) return sub_f32x2(a, b);
+    else return mk<T>(a.x - b.x, a.y - b.y);
+}
+template <typename T> __device__ __forceinline__ cplx<T> cscale(cplx<T> a, T s) {
+    if constexpr (sizeof(T) == 4) return mul_f32x2(a, make_float2(s, s));
+    else return mk<T>(a.x * s, a.y * s);
+}
 template <typename T> __device__ __forceinline__ cplx<T> cconj(cplx<T> a) { return mk<T>(a.x, -a.y); }
 template <typename T> __device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
     return mk<T>(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));

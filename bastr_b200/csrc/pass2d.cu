@@ -25,7 +25,21 @@
 namespace bastr {
 
 // Elements per thread per unit: 64 bytes of data per unit per thread in both precisions.
-template <typename T> struct EptOf { static constexpr int v = sizeof(T) == 8 ? 8 : 16; };
+#ifndef BASTR_EPT_F32
+#define BASTR_EPT_F32 16
+#endif
+#ifndef BASTR_EPT_F64
+#define BASTR_EPT_F64 8
+#endif
+// Minimum resident blocks per SM asked of the register allocator for the 2D passes.
+#ifndef BASTR_MINB_2D
+#define BASTR_MINB_2D 1
+#endif
+template <typename T> struct EptOf { static constexpr int v = sizeof(T) == 8 ? BASTR_EPT_F64 : BASTR_EPT_F32; };
+// The forward y pass (two units, FP64 epilogue) runs best with more, lighter threads.
+#ifndef BASTR_EPT_YFWD_F32
+#define BASTR_EPT_YFWD_F32 8
+#endif
 template <int N, int EPT> constexpr int ept_fit() { return N < EPT ? N : EPT; }
 // Lines handled by one block: at least 128 threads per block.
 template <int NTR> constexpr int groups_per_block() { return NTR >= 128 ? 1 : 128 / NTR; }
@@ -54,12 +68,17 @@ template <typename T, typename TIN, int NY, int SET> struct YInv2D {
     using FFT = RegFFT<T, NY, EPT, UG, true>;
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
-    static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<TIN>);   // one staged group
-    static constexpr size_t SMEM = STAGE + (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr int MINB = BASTR_MINB_2D;
+    static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    // staging of G columns of KY modes x 2 components, sized at run time
+    __host__ __device__ static size_t stage_bytes(int KY) {
+        return ((size_t)G * KY * 2 * sizeof(cplx<TIN>) + 15) & ~(size_t)15;
+    }
+    static size_t smem(int KY) { return stage_bytes(KY) + XCH; }
 };
 
 template <typename T, typename TIN, int NY, int SET>
-__global__ void __launch_bounds__(YInv2D<T, TIN, NY, SET>::NT)
+__global__ void __launch_bounds__(YInv2D<T, TIN, NY, SET>::NT, YInv2D<T, TIN, NY, SET>::MINB)
 k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Geo g,
          const cplx<T>* __restrict__ tw) {
     using P = YInv2D<T, TIN, NY, SET>;
@@ -68,8 +87,8 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<TIN>* stg = reinterpret_cast<cplx<TIN>*>(smraw);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
     const int K = g.K, KY = g.KY;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY)) + gi * FFT::SMEM_ELEMS;
     const int nitems = (K + G - 1) / G;
     const int colbytes = KY * 2 * (int)sizeof(cplx<TIN>);
     auto issue = [&](int item) {
@@ -156,6 +175,7 @@ template <typename T, int NX, int MODE> struct XPass2D {
     static constexpr int NTR = IFFT::NTR;
     static constexpr int G = groups_per_block<NTR>();
     static constexpr int NT = G * NTR;
+    static constexpr int MINB = BASTR_MINB_2D;
     static constexpr int KMAX = NX / 3;
     // one staged group: G rows of K*FIN mixed values, or G rows of 2 physical components
     static constexpr size_t STAGE = MODE == XM_FROM_PHYS ? (size_t)G * 2 * NX * sizeof(double)
@@ -175,7 +195,7 @@ __device__ __forceinline__ cplx<T> pack_at(cplx<T> A, cplx<T> B, bool mirror, bo
 }
 
 template <typename T, int NX, int MODE>
-__global__ void __launch_bounds__(XPass2D<T, NX, MODE>::NT)
+__global__ void __launch_bounds__(XPass2D<T, NX, MODE>::NT, XPass2D<T, NX, MODE>::MINB)
 k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
           const double* __restrict__ phys_in, double* __restrict__ phys_out,
           double* __restrict__ vg_part, Geo g, const cplx<T>* __restrict__ tw) {
@@ -202,7 +222,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
         cp_async_commit();
     };
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    double etamin = 1.0 / 0.0;
+    double divmax = 0.0;
     int item = blockIdx.x;
     if (item < nitems) issue(item);
     for (; item < nitems; item += gridDim.x) {
@@ -281,19 +301,21 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                     v[e] = mk<T>(n1, n2);
                     if constexpr (MODE == XM_RHS_VG) {
                         if (valid) {
-                            // velgrad_calculate2D (solution.F90:1149-1166), accumulated in FP64
+                            // velgrad_calculate2D (solution.F90:1149-1166): per-point terms in the
+                            // compute precision, sums in FP64; eta_min = sqrt(nu/max|theta|) is
+                            // formed once from the largest |theta| (the map is monotone)
                             const cplx<T> l = v[3 * EPT + e], th = v[4 * EPT + e];
-                            const double U1 = u1, U2 = u2, D11 = u1x, D22 = u2y, D12 = u1y, D21 = u2x;
-                            const double div = D11 + D22;
-                            const double uu = U1 * U1 + U2 * U2;
-                            acc[0] += div * div * uu;
-                            acc[1] += (D11 * D11 + D22 * D22 + 2.0 * D12 * D21) * uu;
-                            acc[2] += div * uu;
-                            acc[3] += 2.0 * U1 * div * (double)l.x + 2.0 * U2 * div * (double)l.y + uu * (double)th.x;
-                            acc[4] += nu * (D12 - D21) * (D12 - D21) + nu * div * div;
-                            etamin = fmin(etamin, sqrt(nu / fabs(div)));
-                            acc[5] += uu;
-                            acc[6] += D11 * D11 + D22 * D22;
+                            const T nuT = (T)nu;
+                            const T div = u1x + u2y;
+                            const T uu = u1 * u1 + u2 * u2;
+                            acc[0] += (double)(div * div * uu);
+                            acc[1] += (double)((u1x * u1x + u2y * u2y + (T)2 * u1y * u2x) * uu);
+                            acc[2] += (double)(div * uu);
+                            acc[3] += (double)((T)2 * u1 * div * l.x + (T)2 * u2 * div * l.y + uu * th.x);
+                            acc[4] += (double)(nuT * (u1y - u2x) * (u1y - u2x) + nuT * div * div);
+                            divmax = fmax(divmax, (double)fabs(div));
+                            acc[5] += (double)uu;
+                            acc[6] += (double)(u1x * u1x + u2y * u2y);
                         }
                     }
                 }
@@ -319,11 +341,11 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
         __syncthreads();
         double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
         block_sum<7, NT>(acc, scratch);
-        const double em = block_min<NT>(etamin, scratch);
+        const double dm = -block_min<NT>(-divmax, scratch);
         if (threadIdx.x == 0) {
 #pragma unroll
             for (int i = 0; i < 7; ++i) vg_part[(size_t)blockIdx.x * 8 + i] = acc[i];
-            vg_part[(size_t)blockIdx.x * 8 + 7] = em;
+            vg_part[(size_t)blockIdx.x * 8 + 7] = dm;
         }
     }
 }
@@ -332,10 +354,11 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
 // Pass C: forward transforms along y of kx columns + spectral epilogue.
 // ---------------------------------------------------------------------------------------
 template <typename T, int NY> struct YFwd2D {
-    static constexpr int EPT = ept_fit<NY, EptOf<T>::v>();
+    static constexpr int EPT = ept_fit<NY, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_YFWD_F32>();
     using FFT = RegFFT<T, NY, EPT, 2, false>;
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
+    static constexpr int MINB = NT >= 256 ? 2 : 1;
     static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
@@ -343,7 +366,7 @@ template <typename T, int NY> struct YFwd2D {
 };
 
 template <typename T, int NY, int EPI>
-__global__ void __launch_bounds__(YFwd2D<T, NY>::NT)
+__global__ void __launch_bounds__(YFwd2D<T, NY>::NT, YFwd2D<T, NY>::MINB)
 k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
          const cplx<T>* __restrict__ tw) {
     using P = YFwd2D<T, NY>;

@@ -1,7 +1,7 @@
 // 3D right-hand side as five fused passes (compute_ut3D, solution.F90:865-928, with the RK3/CN
-// combinations of solution.F90:233-301 folded into the last pass).  Every pass reads whole
-// lines straight into the registers of the first transform stage and writes its last stage's
-// registers transposed for the next pass:
+// combinations of solution.F90:233-301 folded into the last pass).  Every pass is a persistent
+// loop over groups of G lines staged through shared memory with cp.async, transformed in
+// registers, and written transposed for the next pass:
 //
 //   A  zinv : lines (kx,ky) along kz of the truncated state -> MA[kx][z][kyi][f]
 //             f = g_c = IFFT_z(u_c^), h_c = IFFT_z(i kz u_c^)       (+ q_c = IFFT_z(kz^2 u_c^),
@@ -19,7 +19,7 @@
 
 namespace bastr {
 
-// The x pass holds six (eight) units at once: 32 bytes per unit per thread.
+// Passes that hold many units at once use 32 bytes per unit per thread.
 template <typename T> struct EptWide { static constexpr int v = sizeof(T) == 8 ? 4 : 8; };
 
 // ---------------------------------------------------------------------------------------
@@ -27,85 +27,107 @@ template <typename T> struct EptWide { static constexpr int v = sizeof(T) == 8 ?
 // ---------------------------------------------------------------------------------------
 enum ZInvSet : int { ZI_STATE = 0, ZI_RHS = 1, ZI_VG = 2 };
 
-template <typename T, int NZ, int SET> struct ZInv3D {
+template <typename T, typename TIN, int NZ, int SET> struct ZInv3D {
     static constexpr int F = SET == ZI_STATE ? 3 : SET == ZI_RHS ? 6 : 4;
     static constexpr int F0 = SET == ZI_VG ? 6 : 0;
     static constexpr int UG = SET == ZI_STATE ? 3 : 2;
     static constexpr int NG = (F + UG - 1) / UG;
-    static constexpr int EPT = ept_fit<NZ, EptOf<T>::v>();
+    static constexpr int EPT = ept_fit<NZ, EptWide<T>::v>();
     using FFT = RegFFT<T, NZ, EPT, UG, true>;
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
-    static constexpr size_t SMEM = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    // staging of G lines of KZ modes x 3 components, sized at run time
+    __host__ __device__ static size_t stage_bytes(int KZ) {
+        return ((size_t)G * KZ * 3 * sizeof(cplx<TIN>) + 15) & ~(size_t)15;
+    }
+    static size_t smem(int KZ) { return stage_bytes(KZ) + XCH; }
 };
 
 template <typename T, typename TIN, int NZ, int SET>
-__global__ void __launch_bounds__(ZInv3D<T, NZ, SET>::NT)
+__global__ void __launch_bounds__(ZInv3D<T, TIN, NZ, SET>::NT)
 k3d_zinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Geo g,
          const cplx<T>* __restrict__ tw) {
-    using P = ZInv3D<T, NZ, SET>;
+    using P = ZInv3D<T, TIN, NZ, SET>;
     using FFT = typename P::FFT;
-    constexpr int EPT = P::EPT, UG = P::UG, F = P::F;
+    constexpr int EPT = P::EPT, UG = P::UG, F = P::F, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<TIN>* stg = reinterpret_cast<cplx<TIN>*>(smraw);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw) + gi * FFT::SMEM_ELEMS;
     const int K = g.K, KY = g.KY, KZ = g.KZ;
-    const int l = blockIdx.x * P::G + gi;   // line = kx*KY + kyi
-    const bool valid = l < K * KY;
-    const int kx = l / KY, kyi = l - kx * KY;
-    const T kxt = (T)kx, kyt = (T)trunc_k(kyi, K, KY);
-#pragma unroll
-    for (int grp = 0; grp < P::NG; ++grp) {
-        cplx<T> v[UG * EPT];
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KZ)) + gi * FFT::SMEM_ELEMS;
+    const int nlines = K * KY;                 // line = kx*KY + kyi
+    const int nitems = (nlines + G - 1) / G;
+    auto issue = [&](int item) {
+        const int l0 = item * G;
+        stage_line(stg, S + (size_t)l0 * KZ * 3, min(G, nlines - l0) * KZ * 3 * (int)sizeof(cplx<TIN>));
+        cp_async_commit();
+    };
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const int l = item * G + gi;
+        const bool valid = l < nlines;
+        const int kx = l / KY, kyi = l - kx * KY;
+        const T kxt = (T)kx, kyt = (T)trunc_k(kyi, K, KY);
+        const cplx<TIN>* line = stg + (size_t)gi * KZ * 3;
+        cplx<T> r[3][EPT];
 #pragma unroll
         for (int e = 0; e < EPT; ++e) {
-            const int p = FFT::in_pos(t, e);
-            const int kzi = pos_trunc(p, K, KZ, NZ);
-            cplx<T> f[UG];
+            const int kzi = pos_trunc(FFT::in_pos(t, e), K, KZ, NZ);
+            const bool on = valid && kzi >= 0;
 #pragma unroll
-            for (int u = 0; u < UG; ++u) f[u] = mk<T>(0, 0);
-            if (valid && kzi >= 0) {
-                const T kz = (T)trunc_k(kzi, K, KZ);
-                const size_t o = ((size_t)l * KZ + kzi) * 3;
+            for (int c = 0; c < 3; ++c) r[c][e] = on ? cvt<cplx<TIN>, cplx<T>>(line[3 * kzi + c]) : mk<T>(0, 0);
+        }
+        __syncthreads();   // the staging buffer is free: fetch the next line group now
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+#pragma unroll
+        for (int grp = 0; grp < P::NG; ++grp) {
+            cplx<T> v[UG * EPT];
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+                const int kzi = pos_trunc(FFT::in_pos(t, e), K, KZ, NZ);
+                const T kz = (T)(kzi >= 0 ? trunc_k(kzi, K, KZ) : 0);
                 if constexpr (SET == ZI_STATE) {
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) f[c] = cvt<cplx<TIN>, cplx<T>>(S[o + c]);
+                    for (int c = 0; c < 3; ++c) v[c * EPT + e] = r[c][e];
                 } else if constexpr (SET == ZI_RHS) {
-                    const cplx<T> a = cvt<cplx<TIN>, cplx<T>>(S[o + grp]);   // component grp
-                    f[0] = a;
-                    f[1] = cscale<T>(cmuli<T>(a), kz);
+                    v[e] = r[grp][e];
+                    v[EPT + e] = cscale<T>(cmuli<T>(r[grp][e]), kz);
                 } else {
                     const T kz2 = kz * kz;
                     if (grp == 0) {
-                        f[0] = cscale<T>(cvt<cplx<TIN>, cplx<T>>(S[o]), kz2);
-                        f[1] = cscale<T>(cvt<cplx<TIN>, cplx<T>>(S[o + 1]), kz2);
+                        v[e] = cscale<T>(r[0][e], kz2);
+                        v[EPT + e] = cscale<T>(r[1][e], kz2);
                     } else {
-                        const cplx<T> a = cvt<cplx<TIN>, cplx<T>>(S[o]);
-                        const cplx<T> b = cvt<cplx<TIN>, cplx<T>>(S[o + 1]);
-                        const cplx<T> c = cvt<cplx<TIN>, cplx<T>>(S[o + 2]);
-                        f[0] = cscale<T>(c, kz2);
+                        v[e] = cscale<T>(r[2][e], kz2);
                         // lap(theta)^ = -i |k|^2 (k . u^)   (solution.F90:1216)
                         const T kk = kxt * kxt + kyt * kyt + kz2;
-                        const cplx<T> dv = cadd<T>(cadd<T>(cscale<T>(a, kxt), cscale<T>(b, kyt)), cscale<T>(c, kz));
-                        f[1] = cscale<T>(cmulni<T>(dv), kk);
+                        const cplx<T> dv = cadd<T>(cadd<T>(cscale<T>(r[0][e], kxt), cscale<T>(r[1][e], kyt)),
+                                                   cscale<T>(r[2][e], kz));
+                        v[EPT + e] = cscale<T>(cmulni<T>(dv), kk);
                     }
                 }
             }
+            FFT::run(v, sm, tw, t);
+            if (valid) {
 #pragma unroll
-            for (int u = 0; u < UG; ++u) v[u * EPT + e] = f[u];
-        }
-        FFT::run(v, sm, tw, t);
-        if (valid) {
+                for (int e = 0; e < EPT; ++e) {
+                    const int z = FFT::out_pos(t, e);
+                    cplx<T>* dst = MA + (((size_t)kx * NZ + z) * KY + kyi) * ftot + P::F0 + grp * UG;
+                    if constexpr (UG == 2) {
+                        st2<T>(dst, v[e], v[EPT + e]);
+                    } else {
 #pragma unroll
-            for (int e = 0; e < EPT; ++e) {
-                const int z = FFT::out_pos(t, e);
-                cplx<T>* dst = MA + (((size_t)kx * NZ + z) * KY + kyi) * ftot + P::F0 + grp * UG;
-#pragma unroll
-                for (int u = 0; u < UG; ++u)
-                    if (grp * UG + u < F) dst[u] = v[u * EPT + e];
+                        for (int u = 0; u < UG; ++u) dst[u] = v[u * EPT + e];
+                    }
+                }
             }
         }
     }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------------------
@@ -118,11 +140,16 @@ template <typename T, int NY, int SET> struct YInv3D {
     static constexpr int F = SET == YB_STATE ? 3 : SET == YB_RHS ? 9 : 13;
     static constexpr int UG = 3;
     static constexpr int NG = (F + UG - 1) / UG;
-    static constexpr int EPT = ept_fit<NY, EptOf<T>::v>();
+    static constexpr int EPT = ept_fit<NY, EptWide<T>::v>();
     using FFT = RegFFT<T, NY, EPT, UG, true>;
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
-    static constexpr size_t SMEM = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    // staging of G lines of KY modes x FIN fields, sized at run time
+    __host__ __device__ static size_t stage_bytes(int KY) {
+        return ((size_t)G * KY * FIN * sizeof(cplx<T>) + 15) & ~(size_t)15;
+    }
+    static size_t smem(int KY) { return stage_bytes(KY) + XCH; }
 };
 
 template <typename T, int NY, int SET>
@@ -130,60 +157,84 @@ __global__ void __launch_bounds__(YInv3D<T, NY, SET>::NT)
 k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const cplx<T>* __restrict__ tw) {
     using P = YInv3D<T, NY, SET>;
     using FFT = typename P::FFT;
-    constexpr int EPT = P::EPT, UG = P::UG, F = P::F, FIN = P::FIN;
+    constexpr int EPT = P::EPT, UG = P::UG, F = P::F, FIN = P::FIN, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw) + gi * FFT::SMEM_ELEMS;
     const int K = g.K, KY = g.KY, NZ = g.nz;
-    const int l = blockIdx.x * P::G + gi;   // line = z*K + kx
-    const bool valid = l < K * NZ;
-    const int z = l / K, kx = l - z * K;
-#pragma unroll
-    for (int grp = 0; grp < P::NG; ++grp) {
-        cplx<T> v[UG * EPT];
-#pragma unroll
-        for (int e = 0; e < EPT; ++e) {
-            const int p = FFT::in_pos(t, e);
-            const int kyi = pos_trunc(p, K, KY, NY);
-            cplx<T> f[UG];
-#pragma unroll
-            for (int u = 0; u < UG; ++u) f[u] = mk<T>(0, 0);
-            if (valid && kyi >= 0) {
-                const T ky = (T)trunc_k(kyi, K, KY);
-                const cplx<T>* src = MA + (((size_t)kx * NZ + z) * KY + kyi) * FIN;
-                if constexpr (SET == YB_STATE) {
-                    f[0] = src[0]; f[1] = src[1]; f[2] = src[2];
-                } else {
-                    if (grp < 3) {   // component grp: G, Dy, Dz
-                        const cplx<T> gc = src[2 * grp], hc = src[2 * grp + 1];
-                        f[0] = gc;
-                        f[1] = cscale<T>(cmuli<T>(gc), ky);
-                        f[2] = hc;
-                    } else if (grp == 3) {
-                        // lap u_c without its kx^2 part (added in pass C): -ky^2 g_c - IFFT_z(kz^2 u_c^)
-                        const T ky2 = ky * ky;
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) f[c] = csub<T>(cscale<T>(src[2 * c], -ky2), src[6 + c]);
-                    } else {
-                        f[0] = src[9];
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < UG; ++u) v[u * EPT + e] = f[u];
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY)) + gi * FFT::SMEM_ELEMS;
+    const int nlines = K * NZ;                 // line = z*K + kx
+    const int nitems = (nlines + G - 1) / G;
+    const int linebytes = KY * FIN * (int)sizeof(cplx<T>);
+    auto issue = [&](int item) {
+        const int l0 = item * G;
+        const int nl = min(G, nlines - l0);
+        for (int j = 0; j < nl; ++j) {
+            const int l = l0 + j, z = l / K, kx = l - z * K;
+            stage_line(stg + (size_t)j * KY * FIN, MA + ((size_t)kx * NZ + z) * KY * FIN, linebytes);
         }
-        FFT::run(v, sm, tw, t);
-        if (valid) {
+        cp_async_commit();
+    };
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const int l = item * G + gi;
+        const bool valid = l < nlines;
+        const int z = l / K, kx = l - z * K;
+        const cplx<T>* line = stg + (size_t)gi * KY * FIN;
+#pragma unroll
+        for (int grp = 0; grp < P::NG; ++grp) {
+            cplx<T> v[UG * EPT];
 #pragma unroll
             for (int e = 0; e < EPT; ++e) {
-                const int y = FFT::out_pos(t, e);
-                cplx<T>* dst = MB + (((size_t)z * NY + y) * K + kx) * F + grp * UG;
+                const int kyi = pos_trunc(FFT::in_pos(t, e), K, KY, NY);
+                cplx<T> f[UG];
 #pragma unroll
-                for (int u = 0; u < UG; ++u)
-                    if (grp * UG + u < F) dst[u] = v[u * EPT + e];
+                for (int u = 0; u < UG; ++u) f[u] = mk<T>(0, 0);
+                if (valid && kyi >= 0) {
+                    const T ky = (T)trunc_k(kyi, K, KY);
+                    const cplx<T>* src = line + (size_t)kyi * FIN;
+                    if constexpr (SET == YB_STATE) {
+                        f[0] = src[0]; f[1] = src[1]; f[2] = src[2];
+                    } else {
+                        if (grp < 3) {   // component grp: G, Dy, Dz
+                            const cplx<T> gc = src[2 * grp], hc = src[2 * grp + 1];
+                            f[0] = gc;
+                            f[1] = cscale<T>(cmuli<T>(gc), ky);
+                            f[2] = hc;
+                        } else if (grp == 3) {
+                            // lap u_c without its kx^2 part (added in pass C): -ky^2 g_c - IFFT_z(kz^2 u_c^)
+                            const T ky2 = ky * ky;
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) f[c] = csub<T>(cscale<T>(src[2 * c], -ky2), src[6 + c]);
+                        } else {
+                            f[0] = src[9];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < UG; ++u) v[u * EPT + e] = f[u];
+            }
+            if (grp == P::NG - 1) {
+                __syncthreads();   // staging buffer consumed: fetch the next line group
+                if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+            }
+            FFT::run(v, sm, tw, t);
+            if (valid) {
+#pragma unroll
+                for (int e = 0; e < EPT; ++e) {
+                    const int y = FFT::out_pos(t, e);
+                    cplx<T>* dst = MB + (((size_t)z * NY + y) * K + kx) * F + grp * UG;
+#pragma unroll
+                    for (int u = 0; u < UG; ++u)
+                        if (grp * UG + u < F) dst[u] = v[u * EPT + e];
+                }
             }
         }
     }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------------------
@@ -200,9 +251,12 @@ template <typename T, int NX, int MODE> struct XPass3D {
     static constexpr int NTR = IFFT::NTR;
     static constexpr int G = groups_per_block<NTR>();
     static constexpr int NT = G * NTR;
-    static constexpr size_t SMEM_FFT = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
-    static constexpr size_t SMEM = SMEM_FFT > (size_t)9 * NT * 8 ? SMEM_FFT : (size_t)9 * NT * 8;
-    static constexpr int BR = G;
+    static constexpr int KMAX = NX / 3;
+    static constexpr size_t STAGE = MODE == X3_FROM_PHYS ? (size_t)G * 3 * NX * sizeof(double)
+                                                          : (size_t)G * KMAX * FIN * sizeof(cplx<T>);
+    static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
+    static constexpr size_t SMEM = STAGE + XCHR;
 };
 
 template <typename T, int NX, int MODE>
@@ -212,148 +266,171 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
     using P = XPass3D<T, NX, MODE>;
     using IFFT = typename P::IFFT;
     using FFFT = typename P::FFFT;
-    constexpr int ZU = P::ZU, EPT = P::EPT, NT = P::NT, NTR = P::NTR, FIN = P::FIN;
+    constexpr int ZU = P::ZU, EPT = P::EPT, NT = P::NT, NTR = P::NTR, FIN = P::FIN, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
+    unsigned char* stg = smraw;
     const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw) + gi * IFFT::SMEM_ELEMS;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * IFFT::SMEM_ELEMS;
     const int K = g.K, NY = g.ny;
     const int rows = NY * g.nz;
     const size_t npts = (size_t)NX * rows;
-    const int row = blockIdx.x * P::G + gi;   // row = z*NY + y
-    const bool valid = row < rows;
-    cplx<T> v[ZU * EPT];
-
-    if constexpr (MODE == X3_FROM_PHYS) {
+    const int nitems = (rows + G - 1) / G;
+    auto issue = [&](int item) {
+        const int r0 = item * G;
+        const int nr = min(G, rows - r0);
+        if constexpr (MODE == X3_FROM_PHYS) {
+            double* d = reinterpret_cast<double*>(stg);
 #pragma unroll
-        for (int e = 0; e < EPT; ++e) {
-            const int x = FFFT::in_pos(t, e);
-            const size_t o = (size_t)row * NX + x;
-            v[e] = valid ? mk<T>((T)phys_in[o], (T)phys_in[npts + o]) : mk<T>(0, 0);
-            v[EPT + e] = valid ? mk<T>((T)phys_in[2 * npts + o], (T)0) : mk<T>(0, 0);
+            for (int c = 0; c < 3; ++c) stage_line(d + (size_t)c * G * NX, phys_in + c * npts + (size_t)r0 * NX, nr * NX * 8);
+        } else {
+            stage_line(stg, MB + (size_t)r0 * K * FIN, nr * K * FIN * (int)sizeof(cplx<T>));
         }
-    } else {
+        cp_async_commit();
+    };
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    double divmax = 0.0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const int row = item * G + gi;   // row = z*NY + y
+        const bool valid = row < rows;
+        cplx<T> v[ZU * EPT];
+        if constexpr (MODE == X3_FROM_PHYS) {
+            const double* d = reinterpret_cast<const double*>(stg) + (size_t)gi * NX;
 #pragma unroll
-        for (int e = 0; e < EPT; ++e) {
-            const int p = IFFT::in_pos(t, e);
-            const bool lo = p < K, hi = p > NX - K;
-            const int k = lo ? p : NX - p;
+            for (int e = 0; e < EPT; ++e) {
+                const int x = FFFT::in_pos(t, e);
+                v[e] = valid ? mk<T>((T)d[x], (T)d[(size_t)G * NX + x]) : mk<T>(0, 0);
+                v[EPT + e] = valid ? mk<T>((T)d[(size_t)2 * G * NX + x], (T)0) : mk<T>(0, 0);
+            }
+        } else {
+            const cplx<T>* rw = reinterpret_cast<const cplx<T>*>(stg) + (size_t)gi * K * FIN;
 #pragma unroll
-            for (int u = 0; u < ZU; ++u) v[u * EPT + e] = mk<T>(0, 0);
-            if (valid && (lo || hi)) {
-                const cplx<T>* src = MB + ((size_t)row * K + k) * FIN;
-                const bool z0 = p == 0;
-                if constexpr (MODE == X3_TO_PHYS) {
-                    v[e] = pack_at<T>(src[0], src[1], hi, z0);
-                    v[EPT + e] = pack_at<T>(src[2], mk<T>(0, 0), hi, z0);
-                } else {
-                    const T kx = (T)k;
-                    const cplx<T> G1 = src[0], Dy1 = src[1], Dz1 = src[2];
-                    const cplx<T> G2 = src[3], Dy2 = src[4], Dz2 = src[5];
-                    const cplx<T> G3 = src[6], Dy3 = src[7], Dz3 = src[8];
-                    const cplx<T> X1 = cscale<T>(cmuli<T>(G1), kx), X2 = cscale<T>(cmuli<T>(G2), kx),
-                                  X3 = cscale<T>(cmuli<T>(G3), kx);
-                    v[e] = pack_at<T>(G1, G2, hi, z0);                 // u1, u2
-                    v[EPT + e] = pack_at<T>(G3, X1, hi, z0);           // u3, du1/dx
-                    v[2 * EPT + e] = pack_at<T>(X2, X3, hi, z0);       // du2/dx, du3/dx
-                    v[3 * EPT + e] = pack_at<T>(Dy1, Dy2, hi, z0);     // du1/dy, du2/dy
-                    v[4 * EPT + e] = pack_at<T>(Dy3, Dz1, hi, z0);     // du3/dy, du1/dz
-                    v[5 * EPT + e] = pack_at<T>(Dz2, Dz3, hi, z0);     // du2/dz, du3/dz
-                    if constexpr (MODE == X3_RHS_VG) {
-                        const T kx2 = kx * kx;
-                        v[6 * EPT + e] = pack_at<T>(csub<T>(src[9], cscale<T>(G1, kx2)),
-                                                    csub<T>(src[10], cscale<T>(G2, kx2)), hi, z0);
-                        v[7 * EPT + e] = pack_at<T>(csub<T>(src[11], cscale<T>(G3, kx2)), src[12], hi, z0);
+            for (int e = 0; e < EPT; ++e) {
+                const int p = IFFT::in_pos(t, e);
+                const bool lo = p < K, hi = p > NX - K;
+                const int k = lo ? p : NX - p;
+#pragma unroll
+                for (int u = 0; u < ZU; ++u) v[u * EPT + e] = mk<T>(0, 0);
+                if (valid && (lo || hi)) {
+                    const cplx<T>* src = rw + (size_t)k * FIN;
+                    const bool z0 = p == 0;
+                    if constexpr (MODE == X3_TO_PHYS) {
+                        v[e] = pack_at<T>(src[0], src[1], hi, z0);
+                        v[EPT + e] = pack_at<T>(src[2], mk<T>(0, 0), hi, z0);
+                    } else {
+                        const T kx = (T)k;
+                        const cplx<T> G1 = src[0], Dy1 = src[1], Dz1 = src[2];
+                        const cplx<T> G2 = src[3], Dy2 = src[4], Dz2 = src[5];
+                        const cplx<T> G3 = src[6], Dy3 = src[7], Dz3 = src[8];
+                        const cplx<T> X1 = cscale<T>(cmuli<T>(G1), kx), X2 = cscale<T>(cmuli<T>(G2), kx),
+                                      X3 = cscale<T>(cmuli<T>(G3), kx);
+                        v[e] = pack_at<T>(G1, G2, hi, z0);                 // u1, u2
+                        v[EPT + e] = pack_at<T>(G3, X1, hi, z0);           // u3, du1/dx
+                        v[2 * EPT + e] = pack_at<T>(X2, X3, hi, z0);       // du2/dx, du3/dx
+                        v[3 * EPT + e] = pack_at<T>(Dy1, Dy2, hi, z0);     // du1/dy, du2/dy
+                        v[4 * EPT + e] = pack_at<T>(Dy3, Dz1, hi, z0);     // du3/dy, du1/dz
+                        v[5 * EPT + e] = pack_at<T>(Dz2, Dz3, hi, z0);     // du2/dz, du3/dz
+                        if constexpr (MODE == X3_RHS_VG) {
+                            const T kx2 = kx * kx;
+                            v[6 * EPT + e] = pack_at<T>(csub<T>(src[9], cscale<T>(G1, kx2)),
+                                                        csub<T>(src[10], cscale<T>(G2, kx2)), hi, z0);
+                            v[7 * EPT + e] = pack_at<T>(csub<T>(src[11], cscale<T>(G3, kx2)), src[12], hi, z0);
+                        }
                     }
                 }
             }
         }
-        IFFT::run(v, sm, tw, t);
-    }
+        __syncthreads();   // the staging buffer is free: fetch the next row group now
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        if constexpr (MODE != X3_FROM_PHYS) IFFT::run(v, sm, tw, t);
 
-    if constexpr (MODE == X3_TO_PHYS) {
-        if (valid) {
+        if constexpr (MODE == X3_TO_PHYS) {
+            if (valid) {
+#pragma unroll
+                for (int e = 0; e < EPT; ++e) {
+                    const int x = IFFT::out_pos(t, e);
+                    const size_t o = (size_t)row * NX + x;
+                    phys_out[o] = (double)v[e].x;
+                    phys_out[npts + o] = (double)v[e].y;
+                    phys_out[2 * npts + o] = (double)v[EPT + e].x;
+                }
+            }
+        } else {
+            if constexpr (MODE == X3_RHS || MODE == X3_RHS_VG) {
+                const double nu = g.nu;
+#pragma unroll
+                for (int e = 0; e < EPT; ++e) {
+                    const cplx<T> z0 = v[e], z1 = v[EPT + e], z2 = v[2 * EPT + e];
+                    const cplx<T> z3 = v[3 * EPT + e], z4 = v[4 * EPT + e], z5 = v[5 * EPT + e];
+                    const T u1 = z0.x, u2 = z0.y, u3 = z1.x;
+                    const T d11 = z1.y, d21 = z2.x, d31 = z2.y;   // d_ij = du_i/dx_j
+                    const T d12 = z3.x, d22 = z3.y, d32 = z4.x;
+                    const T d13 = z4.y, d23 = z5.x, d33 = z5.y;
+                    const T n1 = -u1 * d11 - u2 * d12 - u3 * d13;
+                    const T n2 = -u1 * d21 - u2 * d22 - u3 * d23;
+                    const T n3 = -u1 * d31 - u2 * d32 - u3 * d33;
+                    v[e] = mk<T>(n1, n2);
+                    v[EPT + e] = mk<T>(n3, (T)0);
+                    if constexpr (MODE == X3_RHS_VG) {
+                        if (valid) {
+                            // velgrad_calculate3D (solution.F90:1240-1266): per-point terms in the
+                            // compute precision, sums in FP64, eta_min from the largest |theta|
+                            const cplx<T> z6 = v[6 * EPT + e], z7 = v[7 * EPT + e];
+                            const T nuT = (T)nu;
+                            const T div = d11 + d22 + d33;
+                            const T uu = u1 * u1 + u2 * u2 + u3 * u3;
+                            acc[0] += (double)(div * div * uu);
+                            acc[1] += (double)((d11 * d11 + d22 * d22 + d33 * d33 + (T)2 * d12 * d21 +
+                                                (T)2 * d13 * d31 + (T)2 * d23 * d32) * uu);
+                            acc[2] += (double)(div * uu);
+                            acc[3] += (double)((T)2 * u1 * div * z6.x + (T)2 * u2 * div * z6.y +
+                                               (T)2 * u3 * div * z7.x + uu * z7.y);
+                            acc[4] += (double)(nuT * (d12 - d21) * (d12 - d21) + nuT * (d23 - d32) * (d23 - d32) +
+                                               nuT * (d13 - d31) * (d13 - d31) + nuT * div * div);
+                            divmax = fmax(divmax, (double)fabs(div));
+                            acc[5] += (double)uu;
+                            acc[6] += (double)(d11 * d11 + d22 * d22 + d33 * d33);
+                        }
+                    }
+                }
+            }
+            FFFT::run(v, sm, tw, t);
+            // split: unit 0 -> components 0, 1; unit 1 -> component 2
+            constexpr int US = IFFT::US;
 #pragma unroll
             for (int e = 0; e < EPT; ++e) {
-                const int x = IFFT::out_pos(t, e);
-                const size_t o = (size_t)row * NX + x;
-                phys_out[o] = (double)v[e].x;
-                phys_out[npts + o] = (double)v[e].y;
-                phys_out[2 * npts + o] = (double)v[EPT + e].x;
+                const int x = FFFT::out_pos(t, e);
+                sm[pidx(x)] = v[e];
+                sm[US + pidx(x)] = v[EPT + e];
             }
-        }
-        return;
-    }
-
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    double etamin = 1.0 / 0.0;
-    if constexpr (MODE == X3_RHS || MODE == X3_RHS_VG) {
-        const double nu = g.nu;
-#pragma unroll
-        for (int e = 0; e < EPT; ++e) {
-            const cplx<T> z0 = v[e], z1 = v[EPT + e], z2 = v[2 * EPT + e];
-            const cplx<T> z3 = v[3 * EPT + e], z4 = v[4 * EPT + e], z5 = v[5 * EPT + e];
-            const T u1 = z0.x, u2 = z0.y, u3 = z1.x;
-            const T d11 = z1.y, d21 = z2.x, d31 = z2.y;   // d_ij = du_i/dx_j
-            const T d12 = z3.x, d22 = z3.y, d32 = z4.x;
-            const T d13 = z4.y, d23 = z5.x, d33 = z5.y;
-            const T n1 = -u1 * d11 - u2 * d12 - u3 * d13;
-            const T n2 = -u1 * d21 - u2 * d22 - u3 * d23;
-            const T n3 = -u1 * d31 - u2 * d32 - u3 * d33;
-            v[e] = mk<T>(n1, n2);
-            v[EPT + e] = mk<T>(n3, (T)0);
-            if constexpr (MODE == X3_RHS_VG) {
-                // velgrad_calculate3D (solution.F90:1240-1266), accumulated in FP64
-                const cplx<T> z6 = v[6 * EPT + e], z7 = v[7 * EPT + e];
-                const double U1 = u1, U2 = u2, U3 = u3;
-                const double D11 = d11, D22 = d22, D33 = d33, D12 = d12, D21 = d21, D13 = d13, D31 = d31,
-                             D23 = d23, D32 = d32;
-                const double div = D11 + D22 + D33;
-                const double uu = U1 * U1 + U2 * U2 + U3 * U3;
-                acc[0] += div * div * uu;
-                acc[1] += (D11 * D11 + D22 * D22 + D33 * D33 + 2.0 * D12 * D21 + 2.0 * D13 * D31 +
-                           2.0 * D23 * D32) * uu;
-                acc[2] += div * uu;
-                acc[3] += 2.0 * U1 * div * (double)z6.x + 2.0 * U2 * div * (double)z6.y +
-                          2.0 * U3 * div * (double)z7.x + uu * (double)z7.y;
-                acc[4] += nu * (D12 - D21) * (D12 - D21) + nu * (D23 - D32) * (D23 - D32) +
-                          nu * (D13 - D31) * (D13 - D31) + nu * div * div;
-                etamin = fmin(etamin, sqrt(nu / fabs(div)));
-                acc[5] += uu;
-                acc[6] += D11 * D11 + D22 * D22 + D33 * D33;
+            __syncthreads();
+            if (valid) {
+                const int z_ = row / NY, y = row - z_ * NY;
+                for (int k = t; k < K; k += NTR) {
+                    const int km = k == 0 ? 0 : NX - k;
+                    cplx<T>* dst = MC + (((size_t)z_ * K + k) * NY + y) * 3;
+                    const cplx<T> Z = sm[pidx(k)], Zc = cconj<T>(sm[pidx(km)]);
+                    const cplx<T> W = sm[US + pidx(k)], Wc = cconj<T>(sm[US + pidx(km)]);
+                    dst[0] = cscale<T>(cadd<T>(Z, Zc), (T)0.5);
+                    dst[1] = cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5);
+                    dst[2] = cscale<T>(cadd<T>(W, Wc), (T)0.5);
+                }
             }
         }
     }
-    FFFT::run(v, sm, tw, t);
-    // split: unit 0 -> components 0, 1; unit 1 -> component 2
-    constexpr int US = IFFT::US;
-#pragma unroll
-    for (int e = 0; e < EPT; ++e) {
-        const int x = FFFT::out_pos(t, e);
-        sm[pidx(x)] = v[e];
-        sm[US + pidx(x)] = v[EPT + e];
-    }
-    __syncthreads();
-    if (valid) {
-        const int z_ = row / NY, y = row - z_ * NY;
-        for (int k = t; k < K; k += NTR) {
-            const int km = k == 0 ? 0 : NX - k;
-            cplx<T>* dst = MC + (((size_t)z_ * K + k) * NY + y) * 3;
-            const cplx<T> Z = sm[pidx(k)], Zc = cconj<T>(sm[pidx(km)]);
-            dst[0] = cscale<T>(cadd<T>(Z, Zc), (T)0.5);
-            dst[1] = cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5);
-            const cplx<T> W = sm[US + pidx(k)], Wc = cconj<T>(sm[US + pidx(km)]);
-            dst[2] = cscale<T>(cadd<T>(W, Wc), (T)0.5);
-        }
-    }
+    cp_async_wait<0>();
     if constexpr (MODE == X3_RHS_VG) {
         __syncthreads();
-        double* scratch = reinterpret_cast<double*>(smraw);
+        double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
         block_sum<7, NT>(acc, scratch);
-        const double em = block_min<NT>(etamin, scratch);
+        const double dm = -block_min<NT>(-divmax, scratch);
         if (threadIdx.x == 0) {
 #pragma unroll
             for (int i = 0; i < 7; ++i) vg_part[(size_t)blockIdx.x * 8 + i] = acc[i];
-            vg_part[(size_t)blockIdx.x * 8 + 7] = em;
+            vg_part[(size_t)blockIdx.x * 8 + 7] = dm;
         }
     }
 }
@@ -362,11 +439,12 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
 // Pass D: forward y transforms, truncation to |ky| < K.
 // ---------------------------------------------------------------------------------------
 template <typename T, int NY> struct YFwd3D {
-    static constexpr int EPT = ept_fit<NY, EptOf<T>::v>();
+    static constexpr int EPT = ept_fit<NY, EptWide<T>::v>();
     using FFT = RegFFT<T, NY, EPT, 3, false>;
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
-    static constexpr size_t SMEM = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t STAGE = (size_t)G * NY * 3 * sizeof(cplx<T>);
+    static constexpr size_t SMEM = STAGE + (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
 };
 
 template <typename T, int NY>
@@ -374,47 +452,68 @@ __global__ void __launch_bounds__(YFwd3D<T, NY>::NT)
 k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const cplx<T>* __restrict__ tw) {
     using P = YFwd3D<T, NY>;
     using FFT = typename P::FFT;
-    constexpr int EPT = P::EPT;
+    constexpr int EPT = P::EPT, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw) + gi * FFT::SMEM_ELEMS;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
     const int K = g.K, KY = g.KY, NZ = g.nz;
-    const int l = blockIdx.x * P::G + gi;   // line = kx*NZ + z
-    const bool valid = l < K * NZ;
-    const int kx = l / NZ, z = l - kx * NZ;
-    cplx<T> v[3 * EPT];
-#pragma unroll
-    for (int e = 0; e < EPT; ++e) {
-        const int y = FFT::in_pos(t, e);
-        const cplx<T>* src = MC + (((size_t)z * K + kx) * NY + y) * 3;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) v[c * EPT + e] = valid ? src[c] : mk<T>(0, 0);
-    }
-    FFT::run(v, sm, tw, t);
-    if (valid) {
+    const int nlines = K * NZ;                 // line = kx*NZ + z
+    const int nitems = (nlines + G - 1) / G;
+    auto issue = [&](int item) {
+        const int l0 = item * G;
+        const int nl = min(G, nlines - l0);
+        for (int j = 0; j < nl; ++j) {
+            const int l = l0 + j, kx = l / NZ, z = l - kx * NZ;
+            stage_line(stg + (size_t)j * NY * 3, MC + ((size_t)z * K + kx) * NY * 3, NY * 3 * (int)sizeof(cplx<T>));
+        }
+        cp_async_commit();
+    };
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const int l = item * G + gi;
+        const bool valid = l < nlines;
+        const int kx = l / NZ, z = l - kx * NZ;
+        const cplx<T>* line = stg + (size_t)gi * NY * 3;
+        cplx<T> v[3 * EPT];
 #pragma unroll
         for (int e = 0; e < EPT; ++e) {
-            const int p = FFT::out_pos(t, e);
-            const int kyi = pos_trunc(p, K, KY, NY);
-            if (kyi < 0) continue;
-            cplx<T>* dst = MD + (((size_t)kx * KY + kyi) * NZ + z) * 3;
+            const int y = FFT::in_pos(t, e);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) dst[c] = v[c * EPT + e];
+            for (int c = 0; c < 3; ++c) v[c * EPT + e] = valid ? line[3 * y + c] : mk<T>(0, 0);
+        }
+        __syncthreads();
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        FFT::run(v, sm, tw, t);
+        if (valid) {
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+                const int kyi = pos_trunc(FFT::out_pos(t, e), K, KY, NY);
+                if (kyi < 0) continue;
+                cplx<T>* dst = MD + (((size_t)kx * KY + kyi) * NZ + z) * 3;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) dst[c] = v[c * EPT + e];
+            }
         }
     }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------------------
 // Pass E: forward z transforms + spectral epilogue.
 // ---------------------------------------------------------------------------------------
 template <typename T, int NZ> struct ZFwd3D {
-    static constexpr int EPT = ept_fit<NZ, EptOf<T>::v>();
+    static constexpr int EPT = ept_fit<NZ, EptWide<T>::v>();
     using FFT = RegFFT<T, NZ, EPT, 3, false>;
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
-    static constexpr int L = G;   // lines per block
-    static constexpr size_t SMEM_FFT = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
-    static constexpr size_t SMEM = SMEM_FFT > (size_t)NT * 8 ? SMEM_FFT : (size_t)NT * 8;
+    static constexpr size_t STAGE = (size_t)G * NZ * 3 * sizeof(cplx<T>);
+    static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
+    static constexpr size_t SMEM = STAGE + XCHR;
 };
 
 template <typename T, int NZ, int EPI>
@@ -422,54 +521,69 @@ __global__ void __launch_bounds__(ZFwd3D<T, NZ>::NT)
 k3d_zfwd(const cplx<T>* __restrict__ MD, StageIO<T> io, int input_is_u0, Geo g, const cplx<T>* __restrict__ tw) {
     using P = ZFwd3D<T, NZ>;
     using FFT = typename P::FFT;
-    constexpr int EPT = P::EPT, NT = P::NT;
+    constexpr int EPT = P::EPT, NT = P::NT, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw) + gi * FFT::SMEM_ELEMS;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
     const int K = g.K, KY = g.KY, KZ = g.KZ;
-    const int l = blockIdx.x * P::G + gi;   // line = kx*KY + kyi
-    const bool valid = l < K * KY;
-    const int kx = l / KY, kyi = l - kx * KY;
-    cplx<T> v[3 * EPT];
-#pragma unroll
-    for (int e = 0; e < EPT; ++e) {
-        const int z = FFT::in_pos(t, e);
-        const cplx<T>* src = MD + ((size_t)l * NZ + z) * 3;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) v[c * EPT + e] = valid ? src[c] : mk<T>(0, 0);
-    }
-    FFT::run(v, sm, tw, t);
-
+    const int nlines = K * KY;                 // line = kx*KY + kyi
+    const int nitems = (nlines + G - 1) / G;
+    auto issue = [&](int item) {
+        const int l0 = item * G;
+        stage_line(stg, MD + (size_t)l0 * NZ * 3, min(G, nlines - l0) * NZ * 3 * (int)sizeof(cplx<T>));
+        cp_async_commit();
+    };
     const double inv_n = g.inv_n;
     const long long K2 = (long long)K * K;
     double en = 0.0;
-    if (valid) {
-        const int ky = trunc_k(kyi, K, KY);
-        const double w = kx == 0 ? 1.0 : 2.0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const int l = item * G + gi;
+        const bool valid = l < nlines;
+        const int kx = l / KY, kyi = l - kx * KY;
+        const cplx<T>* line = stg + (size_t)gi * NZ * 3;
+        cplx<T> v[3 * EPT];
 #pragma unroll
         for (int e = 0; e < EPT; ++e) {
-            const int p = FFT::out_pos(t, e);
-            const int kzi = pos_trunc(p, K, KZ, NZ);
-            if (kzi < 0) continue;
-            const int kz = trunc_k(kzi, K, KZ);
-            const size_t o = ((size_t)l * KZ + kzi) * 3;
-            const long long m2i = (long long)kx * kx + (long long)ky * ky + (long long)kz * kz;
-            double2 vv[3];
-            if (m2i < K2) {   // spherical 2/3 rule, tool.F90:206-214
+            const int z = FFT::in_pos(t, e);
 #pragma unroll
-                for (int c = 0; c < 3; ++c) vv[c] = dscale(cvt<cplx<T>, double2>(v[c * EPT + e]), inv_n);
-            } else {
+            for (int c = 0; c < 3; ++c) v[c * EPT + e] = valid ? line[3 * z + c] : mk<T>(0, 0);
+        }
+        __syncthreads();
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        FFT::run(v, sm, tw, t);
+        if (valid) {
+            const int ky = trunc_k(kyi, K, KY);
+            const double w = kx == 0 ? 1.0 : 2.0;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) vv[c] = make_double2(0, 0);
+            for (int e = 0; e < EPT; ++e) {
+                const int kzi = pos_trunc(FFT::out_pos(t, e), K, KZ, NZ);
+                if (kzi < 0) continue;
+                const int kz = trunc_k(kzi, K, KZ);
+                const size_t o = ((size_t)l * KZ + kzi) * 3;
+                const long long m2i = (long long)kx * kx + (long long)ky * ky + (long long)kz * kz;
+                double2 vv[3];
+                if (m2i < K2) {   // spherical 2/3 rule, tool.F90:206-214
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) vv[c] = dscale(cvt<cplx<T>, double2>(v[c * EPT + e]), inv_n);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) vv[c] = make_double2(0, 0);
+                }
+                const double kv[3] = {(double)kx, (double)ky, (double)kz};
+                rk_epilogue<T, 3, EPI>(vv, kv, (double)m2i, o, io, input_is_u0 != 0, g, w, en);
             }
-            const double kv[3] = {(double)kx, (double)ky, (double)kz};
-            rk_epilogue<T, 3, EPI>(vv, kv, (double)m2i, o, io, input_is_u0 != 0, g, w, en);
         }
     }
+    cp_async_wait<0>();
     if constexpr (EPI == EPI_RK3 || EPI == EPI_CN_LAST) {
         if (io.energy_part) {
             __syncthreads();
-            double* scratch = reinterpret_cast<double*>(smraw);
+            double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
             double r[1] = {en};
             block_sum<1, NT>(r, scratch);
             if (threadIdx.x == 0) io.energy_part[blockIdx.x] = r[0];

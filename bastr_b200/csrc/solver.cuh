@@ -144,15 +144,19 @@ __device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double 
         }
         if (g.lproject) {   // projection2D/3D, tool.F90:219-270
             if (m2 > 0.25) {
-                const double kk = sqrt(m2);
+                // u_d = (k/|k|) (k/|k|) . v, with one reciprocal per mode
+                const double ik = 1.0 / sqrt(m2);
+                double kh[D];
+#pragma unroll
+                for (int c = 0; c < D; ++c) kh[c] = k[c] * ik;
                 double2 ud = make_double2(0, 0);
 #pragma unroll
                 for (int c = 0; c < D; ++c) {
-                    ud.x += v[c].x * k[c] / kk;
-                    ud.y += v[c].y * k[c] / kk;
+                    ud.x += v[c].x * kh[c];
+                    ud.y += v[c].y * kh[c];
                 }
 #pragma unroll
-                for (int c = 0; c < D; ++c) v[c] = make_double2(ud.x * k[c] / kk, ud.y * k[c] / kk);
+                for (int c = 0; c < D; ++c) v[c] = make_double2(ud.x * kh[c], ud.y * kh[c]);
             } else {
 #pragma unroll
                 for (int c = 0; c < D; ++c) v[c] = make_double2(0, 0);
@@ -198,13 +202,24 @@ template <int NPEND> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
 }
 
-// Copies `bytes` (a multiple of 16, both ends 16-byte aligned) from global to shared memory with
-// all threads of the block; returns without waiting.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+
+// Copies `bytes` (a multiple of 8, both ends 8-byte aligned) from global to shared memory with
+// all threads of the block, in 16-byte chunks when both ends and the length allow it and in
+// 8-byte chunks otherwise; returns without waiting.
 __device__ __forceinline__ void stage_line(void* smem_dst, const void* gmem_src, int bytes) {
-    const int n16 = bytes >> 4;
     char* d = static_cast<char*>(smem_dst);
     const char* s = static_cast<const char*>(gmem_src);
-    for (int i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(d + 16 * i, s + 16 * i);
+    if ((((unsigned long long)d | (unsigned long long)s | (unsigned long long)bytes) & 15ull) == 0) {
+        const int n16 = bytes >> 4;
+        for (int i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(d + 16 * i, s + 16 * i);
+    } else {
+        const int n8 = bytes >> 3;
+        for (int i = threadIdx.x; i < n8; i += blockDim.x) cp_async8(d + 8 * i, s + 8 * i);
+    }
 }
 
 // Lines (or rows) per block so that one block holds about 48 KB of transform data; a power of 2.
