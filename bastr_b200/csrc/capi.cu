@@ -684,6 +684,7 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     g.nx = p->ia; g.ny = p->ja; g.nz = nz; g.d = d; g.K = K;
     g.KY = 2 * K - 1; g.KZ = d == 3 ? 2 * K - 1 : 1;
     g.lproject = p->lprojectd ? 1 : 0;
+    g.ps = 1;
     g.nu = p->reynolds == 0.0 ? 0.0 : [&] {
         const double tc = 110.4 / p->ref_tem, tc1 = 1.0 + tc;   // miucal(1.d0), solution.F90:1315-1329
         return 1.0 * std::sqrt(1.0) * tc1 / (1.0 + tc);
@@ -711,7 +712,8 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
         h->n_vg_blocks = 1;   // set by the launches (persistent grids)
         h->n_en_blocks = 1;
     } else {
-        h->n_state = (size_t)K * g.KY * g.KZ * 3;
+        g.ps = (((long long)K * g.KY * g.KZ + 31) / 32) * 32;   // component planes, 256-byte aligned
+        h->n_state = (size_t)g.ps * 3;
         size_t ma, mb, mc;
         sizes3d(h, cs, ma, mb, mc);
         dev_alloc(h, &h->ma, ma, st);

@@ -58,8 +58,8 @@ __device__ __forceinline__ void spectra_mode(const double2* __restrict__ U0, con
         ed = (udx * udx + udy * udy) / 2;
     } else {
         const int kzi = kz >= 0 ? kz : kz + g.KZ;
-        const size_t o = (((size_t)kx * g.KY + kyi) * g.KZ + kzi) * 3;
-        const double2 a = U0[o], b = U0[o + 1], c = U0[o + 2];
+        const size_t o = ((size_t)kx * g.KY + kyi) * g.KZ + kzi;
+        const double2 a = U0[o], b = U0[o + g.ps], c = U0[o + 2 * g.ps];
         // solution.F90:1047-1053
         const double udx = a.x * k1 / kk + b.x * k2 / kk + c.x * k3 / kk;
         const double udy = a.y * k1 / kk + b.y * k2 / kk + c.y * k3 / kk;
@@ -358,10 +358,11 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
                             kyv = ky; kzv = tt;
                             const int kyi = kyv >= 0 ? kyv : kyv + g.KY;
                             const int kzi = kzv >= 0 ? kzv : kzv + g.KZ;
-                            o = (((size_t)kx * g.KY + kyi) * g.KZ + kzi) * 3;
+                            o = ((size_t)kx * g.KY + kyi) * g.KZ + kzi;
                         }
                         double2 f[3];
-                        for (int c = 0; c < D; ++c) f[c] = U0[o + c];
+                        const size_t cst = D == 2 ? 1 : (size_t)g.ps;
+                        for (int c = 0; c < D; ++c) f[c] = U0[o + c * cst];
                         if (D == 2 && project2d) {
                             // solution.F90:498-501
                             const double kk = sqrt((double)(rr + (long long)tt * tt));
@@ -378,8 +379,8 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
                             acc[0] += w * e2;
                         } else {
                             for (int c = 0; c < D; ++c) {
-                                double2 u = U0[o + c];
-                                U0[o + c] = make_double2(u.x + factor * f[c].x, u.y + factor * f[c].y);
+                                double2 u = U0[o + c * cst];
+                                U0[o + c * cst] = make_double2(u.x + factor * f[c].x, u.y + factor * f[c].y);
                             }
                         }
                     }

@@ -248,19 +248,20 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
 #pragma unroll
                 for (int u = 0; u < ZU; ++u) v[u * EPT + e] = mk<T>(0, 0);
                 if (valid && (lo || hi)) {
-                    const cplx<T>* src = row + (size_t)k * FIN;
+                    const cplx<T>* src0 = row + (size_t)k * FIN;
+                    auto src = [&](int f) { return src0[f]; };
                     const bool z0 = p == 0;
-                    const cplx<T> g1 = src[0];
+                    const cplx<T> g1 = src(0);
                     if constexpr (MODE == XM_TO_PHYS) {
-                        v[e] = pack_at<T>(g1, src[1], hi, z0);
+                        v[e] = pack_at<T>(g1, src(1), hi, z0);
                     } else {
-                        const cplx<T> h1 = src[1], g2 = src[2], h2 = src[3];
+                        const cplx<T> h1 = src(1), g2 = src(2), h2 = src(3);
                         const T kx = (T)k;
                         v[e] = pack_at<T>(g1, g2, hi, z0);
                         v[EPT + e] = pack_at<T>(cscale<T>(cmuli<T>(g1), kx), cscale<T>(cmuli<T>(g2), kx), hi, z0);
                         v[2 * EPT + e] = pack_at<T>(h1, h2, hi, z0);
                         if constexpr (MODE == XM_RHS_VG) {
-                            const cplx<T> q1 = src[4], q2 = src[5], th = src[6];
+                            const cplx<T> q1 = src(4), q2 = src(5), th = src(6);
                             const T kx2 = kx * kx;
                             v[3 * EPT + e] = pack_at<T>(csub<T>(cscale<T>(g1, -kx2), q1),
                                                         csub<T>(cscale<T>(g2, -kx2), q2), hi, z0);
@@ -424,7 +425,7 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
                     vv[1] = make_double2(0, 0);
                 }
                 const double kv[2] = {(double)kx, (double)ky};
-                rk_epilogue<T, 2, EPI>(vv, kv, (double)m2i, o, io, input_is_u0 != 0, g, w, en);
+                rk_epilogue<T, 2, EPI>(vv, kv, (double)m2i, o, 1, io, input_is_u0 != 0, g, w, en);
             }
         }
     }

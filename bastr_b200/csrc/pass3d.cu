@@ -3,10 +3,10 @@
 // loop over groups of G lines staged through shared memory with cp.async, transformed in
 // registers, and written transposed for the next pass:
 //
-//   A  zinv : lines (kx,ky) along kz of the truncated state -> MA[kx][z][kyi][f]
+//   A  zinv : lines (kx,ky) along kz of the truncated state -> MA[kx][kyi][f][z]
 //             f = g_c = IFFT_z(u_c^), h_c = IFFT_z(i kz u_c^)       (+ q_c = IFFT_z(kz^2 u_c^),
 //             t = IFFT_z(lap(theta)^) when velocity-gradient statistics are due)
-//   B  yinv : lines (kx,z) along ky -> MB[z][y][kx][f]
+//   B  yinv : lines (kx,z) along ky -> MB[z][kx][f][y] (each line's outputs contiguous per field)
 //             f = G_c = IFFT_y(g_c), Dy_c = IFFT_y(i ky g_c), Dz_c = IFFT_y(h_c)  (+ lap u_c, lap theta)
 //   C  xpass: rows (y,z): six packed complex inverse x transforms give u_c and all nine
 //             du_i/dx_j in registers; N_i = -(u_j du_i/dx_j) (solution.F90:903-908); two packed
@@ -37,10 +37,11 @@ template <typename T, typename TIN, int NZ, int SET> struct ZInv3D {
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
-    // staging of G lines of KZ modes x 3 components, sized at run time
-    __host__ __device__ static size_t stage_bytes(int KZ) {
-        return ((size_t)G * KZ * 3 * sizeof(cplx<TIN>) + 15) & ~(size_t)15;
+    // staging of G lines of KZ modes for each of the 3 component planes, sized at run time
+    __host__ __device__ static size_t plane_bytes(int KZ) {
+        return ((size_t)G * KZ * sizeof(cplx<TIN>) + 15) & ~(size_t)15;
     }
+    __host__ __device__ static size_t stage_bytes(int KZ) { return 3 * plane_bytes(KZ); }
     static size_t smem(int KZ) { return stage_bytes(KZ) + XCH; }
 };
 
@@ -58,9 +59,13 @@ k3d_zinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KZ)) + gi * FFT::SMEM_ELEMS;
     const int nlines = K * KY;                 // line = kx*KY + kyi
     const int nitems = (nlines + G - 1) / G;
+    const size_t pe = P::plane_bytes(KZ) / sizeof(cplx<TIN>);   // staged elements per plane
     auto issue = [&](int item) {
         const int l0 = item * G;
-        stage_line(stg, S + (size_t)l0 * KZ * 3, min(G, nlines - l0) * KZ * 3 * (int)sizeof(cplx<TIN>));
+        const int nl = min(G, nlines - l0);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            stage_line(stg + c * pe, S + c * g.ps + (size_t)l0 * KZ, nl * KZ * (int)sizeof(cplx<TIN>));
         cp_async_commit();
     };
     int item = blockIdx.x;
@@ -72,14 +77,14 @@ k3d_zinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
         const bool valid = l < nlines;
         const int kx = l / KY, kyi = l - kx * KY;
         const T kxt = (T)kx, kyt = (T)trunc_k(kyi, K, KY);
-        const cplx<TIN>* line = stg + (size_t)gi * KZ * 3;
+        const cplx<TIN>* line = stg + (size_t)gi * KZ;
         cplx<T> r[3][EPT];
 #pragma unroll
         for (int e = 0; e < EPT; ++e) {
             const int kzi = pos_trunc(FFT::in_pos(t, e), K, KZ, NZ);
             const bool on = valid && kzi >= 0;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) r[c][e] = on ? cvt<cplx<TIN>, cplx<T>>(line[3 * kzi + c]) : mk<T>(0, 0);
+            for (int c = 0; c < 3; ++c) r[c][e] = on ? cvt<cplx<TIN>, cplx<T>>(line[c * pe + kzi]) : mk<T>(0, 0);
         }
         __syncthreads();   // the staging buffer is free: fetch the next line group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
@@ -113,15 +118,13 @@ k3d_zinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
             }
             FFT::run(v, sm, tw, t);
             if (valid) {
+                // MA[kx][kyi][f][z]: each line's field is a contiguous run along z
+                cplx<T>* dst = MA + ((size_t)l * ftot + P::F0 + grp * UG) * NZ;
 #pragma unroll
-                for (int e = 0; e < EPT; ++e) {
-                    const int z = FFT::out_pos(t, e);
-                    cplx<T>* dst = MA + (((size_t)kx * NZ + z) * KY + kyi) * ftot + P::F0 + grp * UG;
-                    if constexpr (UG == 2) {
-                        st2<T>(dst, v[e], v[EPT + e]);
-                    } else {
+                for (int u = 0; u < UG; ++u) {
+                    if (grp * UG + u < F) {
 #pragma unroll
-                        for (int u = 0; u < UG; ++u) dst[u] = v[u * EPT + e];
+                        for (int e = 0; e < EPT; ++e) dst[(size_t)u * NZ + FFT::out_pos(t, e)] = v[u * EPT + e];
                     }
                 }
             }
@@ -142,10 +145,11 @@ template <typename T, int NY, int SET> struct YInv3D {
     static constexpr int NG = (F + UG - 1) / UG;
     static constexpr int EPT = ept_fit<NY, EptWide<T>::v>();
     using FFT = RegFFT<T, NY, EPT, UG, true>;
-    static constexpr int G = groups_per_block<FFT::NTR>();
+    // lines of one block: consecutive z of one kx (every extent is a power of two >= 16)
+    static constexpr int G = groups_per_block<FFT::NTR>() > 16 ? 16 : groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
-    // staging of G lines of KY modes x FIN fields, sized at run time
+    // staging [kyi][f][line] of KY modes x FIN fields, sized at run time
     __host__ __device__ static size_t stage_bytes(int KY) {
         return ((size_t)G * KY * FIN * sizeof(cplx<T>) + 15) & ~(size_t)15;
     }
@@ -163,15 +167,22 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
     const int K = g.K, KY = g.KY, NZ = g.nz;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY)) + gi * FFT::SMEM_ELEMS;
-    const int nlines = K * NZ;                 // line = z*K + kx
+    const int nlines = K * NZ;                 // line = kx*NZ + z
     const int nitems = (nlines + G - 1) / G;
-    const int linebytes = KY * FIN * (int)sizeof(cplx<T>);
     auto issue = [&](int item) {
-        const int l0 = item * G;
-        const int nl = min(G, nlines - l0);
-        for (int j = 0; j < nl; ++j) {
-            const int l = l0 + j, z = l / K, kx = l - z * K;
-            stage_line(stg + (size_t)j * KY * FIN, MA + ((size_t)kx * NZ + z) * KY * FIN, linebytes);
+        // gather [kyi][f][z] from MA[kx][kyi][f][z]: G consecutive z per (kyi, f)
+        const int l0 = item * G, kx0 = l0 / NZ, z0 = l0 - kx0 * NZ;
+        constexpr int RB = G * (int)sizeof(cplx<T>);
+        constexpr int CH = RB % 16 == 0 ? 16 : 8;
+        constexpr int NCH = RB / CH;
+        const int total = KY * FIN * NCH;
+        char* d = reinterpret_cast<char*>(stg);
+        const char* src = reinterpret_cast<const char*>(MA + (size_t)kx0 * KY * FIN * NZ + z0);
+        for (int i = threadIdx.x; i < total; i += P::NT) {
+            const int kf = i / NCH, c = i - kf * NCH;
+            const char* sp = src + (size_t)kf * NZ * sizeof(cplx<T>) + c * CH;
+            if constexpr (CH == 16) cp_async16(d + (size_t)kf * RB + c * CH, sp);
+            else cp_async8(d + (size_t)kf * RB + c * CH, sp);
         }
         cp_async_commit();
     };
@@ -182,8 +193,9 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
         __syncthreads();
         const int l = item * G + gi;
         const bool valid = l < nlines;
-        const int z = l / K, kx = l - z * K;
-        const cplx<T>* line = stg + (size_t)gi * KY * FIN;
+        const int kx = l / NZ, z = l - kx * NZ;
+        // field f of mode kyi for this line at stg[(kyi*FIN + f)*G + gi]
+        const cplx<T>* line = stg + gi;
 #pragma unroll
         for (int grp = 0; grp < P::NG; ++grp) {
             cplx<T> v[UG * EPT];
@@ -195,12 +207,13 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
                 for (int u = 0; u < UG; ++u) f[u] = mk<T>(0, 0);
                 if (valid && kyi >= 0) {
                     const T ky = (T)trunc_k(kyi, K, KY);
-                    const cplx<T>* src = line + (size_t)kyi * FIN;
+                    const cplx<T>* src0 = line + (size_t)kyi * FIN * G;
+                    auto src = [&](int fi) { return src0[fi * G]; };
                     if constexpr (SET == YB_STATE) {
-                        f[0] = src[0]; f[1] = src[1]; f[2] = src[2];
+                        f[0] = src(0); f[1] = src(1); f[2] = src(2);
                     } else {
                         if (grp < 3) {   // component grp: G, Dy, Dz
-                            const cplx<T> gc = src[2 * grp], hc = src[2 * grp + 1];
+                            const cplx<T> gc = src(2 * grp), hc = src(2 * grp + 1);
                             f[0] = gc;
                             f[1] = cscale<T>(cmuli<T>(gc), ky);
                             f[2] = hc;
@@ -208,9 +221,9 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
                             // lap u_c without its kx^2 part (added in pass C): -ky^2 g_c - IFFT_z(kz^2 u_c^)
                             const T ky2 = ky * ky;
 #pragma unroll
-                            for (int c = 0; c < 3; ++c) f[c] = csub<T>(cscale<T>(src[2 * c], -ky2), src[6 + c]);
+                            for (int c = 0; c < 3; ++c) f[c] = csub<T>(cscale<T>(src(2 * c), -ky2), src(6 + c));
                         } else {
-                            f[0] = src[9];
+                            f[0] = src(9);
                         }
                     }
                 }
@@ -223,13 +236,13 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
             }
             FFT::run(v, sm, tw, t);
             if (valid) {
+                cplx<T>* dst = MB + ((size_t)(z * K + kx) * F + grp * UG) * NY;
 #pragma unroll
-                for (int e = 0; e < EPT; ++e) {
-                    const int y = FFT::out_pos(t, e);
-                    cplx<T>* dst = MB + (((size_t)z * NY + y) * K + kx) * F + grp * UG;
+                for (int u = 0; u < UG; ++u) {
+                    if (grp * UG + u < F) {
 #pragma unroll
-                    for (int u = 0; u < UG; ++u)
-                        if (grp * UG + u < F) dst[u] = v[u * EPT + e];
+                        for (int e = 0; e < EPT; ++e) dst[(size_t)u * NY + FFT::out_pos(t, e)] = v[u * EPT + e];
+                    }
                 }
             }
         }
@@ -249,14 +262,16 @@ template <typename T, int NX, int MODE> struct XPass3D {
     using IFFT = RegFFT<T, NX, EPT, ZU, true>;
     using FFFT = RegFFT<T, NX, EPT, 2, false>;
     static constexpr int NTR = IFFT::NTR;
-    static constexpr int G = groups_per_block<NTR>();
+    // rows of one block: consecutive y of one z plane (every extent is a power of two >= 16)
+    static constexpr int G = groups_per_block<NTR>() > 16 ? 16 : groups_per_block<NTR>();
     static constexpr int NT = G * NTR;
     static constexpr int KMAX = NX / 3;
     static constexpr size_t STAGE = MODE == X3_FROM_PHYS ? (size_t)G * 3 * NX * sizeof(double)
                                                           : (size_t)G * KMAX * FIN * sizeof(cplx<T>);
+    static constexpr size_t TILE = (size_t)KMAX * G * 3 * sizeof(cplx<T>);   // output tile [kx][row][c]
     static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
-    static constexpr size_t SMEM = STAGE + XCHR;
+    static constexpr size_t SMEM = STAGE + TILE + XCHR;
 };
 
 template <typename T, int NX, int MODE>
@@ -269,21 +284,34 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
     constexpr int ZU = P::ZU, EPT = P::EPT, NT = P::NT, NTR = P::NTR, FIN = P::FIN, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char* stg = smraw;
+    cplx<T>* tile = reinterpret_cast<cplx<T>*>(smraw + P::STAGE);
     const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * IFFT::SMEM_ELEMS;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::TILE) + gi * IFFT::SMEM_ELEMS;
     const int K = g.K, NY = g.ny;
     const int rows = NY * g.nz;
     const size_t npts = (size_t)NX * rows;
     const int nitems = (rows + G - 1) / G;
     auto issue = [&](int item) {
-        const int r0 = item * G;
-        const int nr = min(G, rows - r0);
+        const int r0 = item * G;   // G consecutive y rows of one z plane
         if constexpr (MODE == X3_FROM_PHYS) {
             double* d = reinterpret_cast<double*>(stg);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) stage_line(d + (size_t)c * G * NX, phys_in + c * npts + (size_t)r0 * NX, nr * NX * 8);
+            for (int c = 0; c < 3; ++c) stage_line(d + (size_t)c * G * NX, phys_in + c * npts + (size_t)r0 * NX, G * NX * 8);
         } else {
-            stage_line(stg, MB + (size_t)r0 * K * FIN, nr * K * FIN * (int)sizeof(cplx<T>));
+            // gather [kx][f][row] from MB[z][kx][f][y]: G consecutive y per (kx, f)
+            const int z0 = r0 / NY, y0 = r0 - z0 * NY;
+            constexpr int RB = G * (int)sizeof(cplx<T>);           // bytes per (kx, f)
+            constexpr int CH = RB % 16 == 0 ? 16 : 8;              // copy granule
+            constexpr int NCH = RB / CH;
+            const int total = K * FIN * NCH;
+            char* d = reinterpret_cast<char*>(stg);
+            const char* src = reinterpret_cast<const char*>(MB + (size_t)z0 * K * FIN * NY + y0);
+            for (int i = threadIdx.x; i < total; i += NT) {
+                const int kf = i / NCH, c = i - kf * NCH;
+                const char* sp = src + ((size_t)kf * NY * sizeof(cplx<T>)) + c * CH;
+                if constexpr (CH == 16) cp_async16(d + (size_t)kf * RB + c * CH, sp);
+                else cp_async8(d + (size_t)kf * RB + c * CH, sp);
+            }
         }
         cp_async_commit();
     };
@@ -306,7 +334,8 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
                 v[EPT + e] = valid ? mk<T>((T)d[(size_t)2 * G * NX + x], (T)0) : mk<T>(0, 0);
             }
         } else {
-            const cplx<T>* rw = reinterpret_cast<const cplx<T>*>(stg) + (size_t)gi * K * FIN;
+            // staged as [kx][f][row]: field f of wavenumber k for this row at (k*FIN + f)*G + gi
+            const cplx<T>* rw = reinterpret_cast<const cplx<T>*>(stg) + gi;
 #pragma unroll
             for (int e = 0; e < EPT; ++e) {
                 const int p = IFFT::in_pos(t, e);
@@ -315,16 +344,17 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
 #pragma unroll
                 for (int u = 0; u < ZU; ++u) v[u * EPT + e] = mk<T>(0, 0);
                 if (valid && (lo || hi)) {
-                    const cplx<T>* src = rw + (size_t)k * FIN;
+                    const cplx<T>* src0 = rw + (size_t)k * FIN * G;
+                    auto src = [&](int f) { return src0[f * G]; };
                     const bool z0 = p == 0;
                     if constexpr (MODE == X3_TO_PHYS) {
-                        v[e] = pack_at<T>(src[0], src[1], hi, z0);
-                        v[EPT + e] = pack_at<T>(src[2], mk<T>(0, 0), hi, z0);
+                        v[e] = pack_at<T>(src(0), src(1), hi, z0);
+                        v[EPT + e] = pack_at<T>(src(2), mk<T>(0, 0), hi, z0);
                     } else {
                         const T kx = (T)k;
-                        const cplx<T> G1 = src[0], Dy1 = src[1], Dz1 = src[2];
-                        const cplx<T> G2 = src[3], Dy2 = src[4], Dz2 = src[5];
-                        const cplx<T> G3 = src[6], Dy3 = src[7], Dz3 = src[8];
+                        const cplx<T> G1 = src(0), Dy1 = src(1), Dz1 = src(2);
+                        const cplx<T> G2 = src(3), Dy2 = src(4), Dz2 = src(5);
+                        const cplx<T> G3 = src(6), Dy3 = src(7), Dz3 = src(8);
                         const cplx<T> X1 = cscale<T>(cmuli<T>(G1), kx), X2 = cscale<T>(cmuli<T>(G2), kx),
                                       X3 = cscale<T>(cmuli<T>(G3), kx);
                         v[e] = pack_at<T>(G1, G2, hi, z0);                 // u1, u2
@@ -335,9 +365,9 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
                         v[5 * EPT + e] = pack_at<T>(Dz2, Dz3, hi, z0);     // du2/dz, du3/dz
                         if constexpr (MODE == X3_RHS_VG) {
                             const T kx2 = kx * kx;
-                            v[6 * EPT + e] = pack_at<T>(csub<T>(src[9], cscale<T>(G1, kx2)),
-                                                        csub<T>(src[10], cscale<T>(G2, kx2)), hi, z0);
-                            v[7 * EPT + e] = pack_at<T>(csub<T>(src[11], cscale<T>(G3, kx2)), src[12], hi, z0);
+                            v[6 * EPT + e] = pack_at<T>(csub<T>(src(9), cscale<T>(G1, kx2)),
+                                                        csub<T>(src(10), cscale<T>(G2, kx2)), hi, z0);
+                            v[7 * EPT + e] = pack_at<T>(csub<T>(src(11), cscale<T>(G3, kx2)), src(12), hi, z0);
                         }
                     }
                 }
@@ -407,24 +437,28 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
                 sm[US + pidx(x)] = v[EPT + e];
             }
             __syncthreads();
-            if (valid) {
-                const int z_ = row / NY, y = row - z_ * NY;
-                for (int k = t; k < K; k += NTR) {
-                    const int km = k == 0 ? 0 : NX - k;
-                    cplx<T>* dst = MC + (((size_t)z_ * K + k) * NY + y) * 3;
-                    const cplx<T> Z = sm[pidx(k)], Zc = cconj<T>(sm[pidx(km)]);
-                    const cplx<T> W = sm[US + pidx(k)], Wc = cconj<T>(sm[US + pidx(km)]);
-                    dst[0] = cscale<T>(cadd<T>(Z, Zc), (T)0.5);
-                    dst[1] = cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5);
-                    dst[2] = cscale<T>(cadd<T>(W, Wc), (T)0.5);
-                }
+            for (int k = t; k < K; k += NTR) {
+                const int km = k == 0 ? 0 : NX - k;
+                cplx<T>* dst = tile + ((size_t)k * G + gi) * 3;
+                const cplx<T> Z = sm[pidx(k)], Zc = cconj<T>(sm[pidx(km)]);
+                const cplx<T> W = sm[US + pidx(k)], Wc = cconj<T>(sm[US + pidx(km)]);
+                dst[0] = cscale<T>(cadd<T>(Z, Zc), (T)0.5);
+                dst[1] = cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5);
+                dst[2] = cscale<T>(cadd<T>(W, Wc), (T)0.5);
+            }
+            __syncthreads();
+            // MC[z][kx][y][c]: the block's G rows of one kx are G*3 contiguous values
+            const int r0 = item * G, z0 = r0 / NY, y0 = r0 - z0 * NY;
+            for (int i = threadIdx.x; i < K * G * 3; i += NT) {
+                const int k = i / (G * 3), rem = i - k * (G * 3);
+                MC[(((size_t)z0 * K + k) * NY + y0) * 3 + rem] = tile[i];
             }
         }
     }
     cp_async_wait<0>();
     if constexpr (MODE == X3_RHS_VG) {
         __syncthreads();
-        double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
+        double* scratch = reinterpret_cast<double*>(smraw + P::STAGE + P::TILE);
         block_sum<7, NT>(acc, scratch);
         const double dm = -block_min<NT>(-divmax, scratch);
         if (threadIdx.x == 0) {
@@ -441,10 +475,12 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
 template <typename T, int NY> struct YFwd3D {
     static constexpr int EPT = ept_fit<NY, EptWide<T>::v>();
     using FFT = RegFFT<T, NY, EPT, 3, false>;
-    static constexpr int G = groups_per_block<FFT::NTR>();
+    // lines of one block: consecutive z of one kx (every extent is a power of two >= 16)
+    static constexpr int G = groups_per_block<FFT::NTR>() > 16 ? 16 : groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
     static constexpr size_t STAGE = (size_t)G * NY * 3 * sizeof(cplx<T>);
-    static constexpr size_t SMEM = STAGE + (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t TILE = (size_t)NY * G * 3 * sizeof(cplx<T>);   // output tile [kyi][line][c]
+    static constexpr size_t SMEM = STAGE + TILE + (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
 };
 
 template <typename T, int NY>
@@ -455,8 +491,9 @@ k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const 
     constexpr int EPT = P::EPT, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* tile = reinterpret_cast<cplx<T>*>(smraw + P::STAGE);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::TILE) + gi * FFT::SMEM_ELEMS;
     const int K = g.K, KY = g.KY, NZ = g.nz;
     const int nlines = K * NZ;                 // line = kx*NZ + z
     const int nitems = (nlines + G - 1) / G;
@@ -488,14 +525,21 @@ k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const 
         __syncthreads();
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
         FFT::run(v, sm, tw, t);
-        if (valid) {
 #pragma unroll
-            for (int e = 0; e < EPT; ++e) {
-                const int kyi = pos_trunc(FFT::out_pos(t, e), K, KY, NY);
-                if (kyi < 0) continue;
-                cplx<T>* dst = MD + (((size_t)kx * KY + kyi) * NZ + z) * 3;
+        for (int e = 0; e < EPT; ++e) {
+            const int kyi = pos_trunc(FFT::out_pos(t, e), K, KY, NY);
+            if (kyi < 0) continue;
+            cplx<T>* dst = tile + ((size_t)kyi * G + gi) * 3;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) dst[c] = v[c * EPT + e];
+            for (int c = 0; c < 3; ++c) dst[c] = v[c * EPT + e];
+        }
+        __syncthreads();
+        // MD[kx][kyi][z][c]: the block's G lines of one kx are G*3 contiguous values per kyi
+        {
+            const int l0 = item * G, kx0 = l0 / NZ, z0 = l0 - kx0 * NZ;
+            for (int i = threadIdx.x; i < KY * G * 3; i += P::NT) {
+                const int kyi = i / (G * 3), rem = i - kyi * (G * 3);
+                MD[(((size_t)kx0 * KY + kyi) * NZ + z0) * 3 + rem] = tile[i];
             }
         }
     }
@@ -564,7 +608,7 @@ k3d_zfwd(const cplx<T>* __restrict__ MD, StageIO<T> io, int input_is_u0, Geo g, 
                 const int kzi = pos_trunc(FFT::out_pos(t, e), K, KZ, NZ);
                 if (kzi < 0) continue;
                 const int kz = trunc_k(kzi, K, KZ);
-                const size_t o = ((size_t)l * KZ + kzi) * 3;
+                const size_t o = (size_t)l * KZ + kzi;   // component planes g.ps apart
                 const long long m2i = (long long)kx * kx + (long long)ky * ky + (long long)kz * kz;
                 double2 vv[3];
                 if (m2i < K2) {   // spherical 2/3 rule, tool.F90:206-214
@@ -575,7 +619,7 @@ k3d_zfwd(const cplx<T>* __restrict__ MD, StageIO<T> io, int input_is_u0, Geo g, 
                     for (int c = 0; c < 3; ++c) vv[c] = make_double2(0, 0);
                 }
                 const double kv[3] = {(double)kx, (double)ky, (double)kz};
-                rk_epilogue<T, 3, EPI>(vv, kv, (double)m2i, o, io, input_is_u0 != 0, g, w, en);
+                rk_epilogue<T, 3, EPI>(vv, kv, (double)m2i, o, (size_t)g.ps, io, input_is_u0 != 0, g, w, en);
             }
         }
     }

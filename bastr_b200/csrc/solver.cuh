@@ -5,8 +5,8 @@
 // every mode with |k| >= K = floor(ia/3); the state and every right-hand side therefore live
 // on kx in [0,K), ky and kz in (-K,K).  Those are the only modes kept in HBM:
 //
-//   S[kx][kyi][c]          2D, kyi in [0,KY), KY = 2K-1, c = velocity component
-//   S[kx][kyi][kzi][c]     3D, kzi in [0,KZ), KZ = 2K-1
+//   S[kx][kyi][c]          2D, kyi in [0,KY), KY = 2K-1, c = velocity component (interleaved)
+//   S[c][kx][kyi][kzi]     3D, kzi in [0,KZ), KZ = 2K-1, component planes ps elements apart
 //
 // with index i < K meaning wavenumber i and i >= K meaning i - (2K-1) (negative side).
 // Modes outside this set are exactly zero in the reference's arithmetic up to round-off.
@@ -21,6 +21,7 @@ struct Geo {
     int K;              // dealias cutoff floor(nx/3); kept kx in [0,K)
     int KY, KZ;         // truncated counts along y and z: 2K-1 (KZ == 1 in 2D)
     int lproject;       // dilatational projection on the right-hand side
+    long long ps;       // 3D: stride between the component planes of a spectral field (elements)
     double nu, dt;
     double inv_n;       // 1 / (nx*ny*nz)
 };
@@ -124,21 +125,22 @@ __device__ __forceinline__ double2 dscale(double2 a, double s) { return make_dou
 // Spectral epilogue of one mode (compute_ut, solution.F90:841-861 / 903-926, and the time
 // integrators, solution.F90:172-301).  v[c] holds the dealiased, 1/N-normalised transform of
 // the advective product; k[c] the wavenumbers, m2 = |k|^2; o the state offset of component 0;
-// w the Hermitian weight of the mode (1 on kx = 0, else 2); en accumulates w*|u0_new|^2.
+// cst the stride between components; w the Hermitian weight of the mode (1 on kx = 0, else 2);
+// en accumulates w*|u0_new|^2.
 template <typename T, int D, int EPI>
-__device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double m2, size_t o,
+__device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double m2, size_t o, size_t cst,
                                             const StageIO<T>& io, bool from_u0, const Geo& g,
                                             double w, double& en) {
     if constexpr (EPI == EPI_STORE) {
 #pragma unroll
-        for (int c = 0; c < D; ++c) io.u0[o + c] = v[c];
+        for (int c = 0; c < D; ++c) io.u0[o + c * cst] = v[c];
         return;
     } else {
         const double nu = g.nu, dt = g.dt;
 #pragma unroll
         for (int c = 0; c < D; ++c) {
             // + nu * FFT(lap u) with lap u^ = -|k|^2 u^
-            const double2 s = ld_stage<T>(io, o + c, from_u0);
+            const double2 s = ld_stage<T>(io, o + c * cst, from_u0);
             v[c].x += nu * (-(s.x * m2));
             v[c].y += nu * (-(s.y * m2));
         }
@@ -165,26 +167,26 @@ __device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double 
         const double dt2 = 2.0 * dt;
 #pragma unroll
         for (int c = 0; c < D; ++c) {
-            const double2 a = io.u0[o + c];
+            const double2 a = io.u0[o + c * cst];
             if constexpr (EPI == EPI_RK1) {
-                io.acc[o + c] = cvt<double2, cplx<T>>(v[c]);
-                io.us[o + c] = cvt<double2, cplx<T>>(make_double2(a.x + dt * v[c].x / 2.0, a.y + dt * v[c].y / 2.0));
+                io.acc[o + c * cst] = cvt<double2, cplx<T>>(v[c]);
+                io.us[o + c * cst] = cvt<double2, cplx<T>>(make_double2(a.x + dt * v[c].x / 2.0, a.y + dt * v[c].y / 2.0));
             } else if constexpr (EPI == EPI_RK2) {
-                const double2 p = cvt<cplx<T>, double2>(io.acc[o + c]);
-                io.us[o + c] = cvt<double2, cplx<T>>(
+                const double2 p = cvt<cplx<T>, double2>(io.acc[o + c * cst]);
+                io.us[o + c * cst] = cvt<double2, cplx<T>>(
                     make_double2(a.x - dt * p.x + dt2 * v[c].x, a.y - dt * p.y + dt2 * v[c].y));
-                io.acc[o + c] = cvt<double2, cplx<T>>(make_double2(p.x + 4.0 * v[c].x, p.y + 4.0 * v[c].y));
+                io.acc[o + c * cst] = cvt<double2, cplx<T>>(make_double2(p.x + 4.0 * v[c].x, p.y + 4.0 * v[c].y));
             } else if constexpr (EPI == EPI_RK3) {
-                const double2 p = cvt<cplx<T>, double2>(io.acc[o + c]);
+                const double2 p = cvt<cplx<T>, double2>(io.acc[o + c * cst]);
                 const double2 n = make_double2(a.x + dt * (p.x + v[c].x) / 6.0, a.y + dt * (p.y + v[c].y) / 6.0);
-                io.u0[o + c] = n;
+                io.u0[o + c * cst] = n;
                 en += w * (n.x * n.x + n.y * n.y);
             } else if constexpr (EPI == EPI_CN_MID) {
-                io.us[o + c] = cvt<double2, cplx<T>>(
+                io.us[o + c * cst] = cvt<double2, cplx<T>>(
                     make_double2(0.5 * ((a.x + dt * v[c].x) + a.x), 0.5 * ((a.y + dt * v[c].y) + a.y)));
             } else if constexpr (EPI == EPI_CN_LAST) {
                 const double2 n = make_double2(a.x + dt * v[c].x, a.y + dt * v[c].y);
-                io.u0[o + c] = n;
+                io.u0[o + c * cst] = n;
                 en += w * (n.x * n.x + n.y * n.y);
             }
         }
