@@ -246,25 +246,39 @@ def cpu_baseline(wl, max_seconds=20.0):
                       f"after 1 warm-up step"}
 
 
+def whole_job_value(steps, ms_max, n_gpus):
+    """Steps/s of the whole job: every replica ran ``steps`` steps; ``ms_max`` is the slowest
+    rank's device time, so the job's throughput is n_gpus * steps over that time."""
+    return n_gpus * steps / (ms_max * 1e-3)
+
+
 class DistCtx:
-    def __init__(self):
+    """One process per GPU (torchrun env): barrier and max-over-ranks of the device times.
+    ``backend="gloo"`` runs the same host logic on CPU processes."""
+
+    def __init__(self, backend="nccl"):
         import datetime
         import torch
         import torch.distributed as dist
         self.dist = dist
         self.torch = torch
+        self.backend = backend
         self.rank = int(os.environ.get("RANK", 0))
         self.world = int(os.environ.get("WORLD_SIZE", 1))
         self.local = int(os.environ.get("LOCAL_RANK", 0))
-        torch.cuda.set_device(self.local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", self.local))
+        if backend == "nccl":
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
 
     def barrier(self):
         self.dist.barrier()
 
     def max(self, v):
-        t = self.torch.tensor([v], dtype=self.torch.float64, device="cuda")
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([v], dtype=self.torch.float64, device=dev)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -285,7 +299,7 @@ def ours(args):
     sampler = ClockSampler(device) if rank == 0 else None
     s, u, stream, ms, clocks, info = measure(wl, prec, args.steps, args.warmup, device, dist_ctx, sampler)
     steps_per_s = args.steps / (ms * 1e-3)
-    value = steps_per_s * n_gpus
+    value = whole_job_value(args.steps, ms, n_gpus)
     roof, shares = kernel_roofline(s, min(args.steps, 20), peak, peak_kind, wl, prec)
     s.close()
     variants = []
