@@ -3,12 +3,16 @@
 // last pass).
 //
 //   A  yinv : per kx column, inverse y transforms of the truncated spectrum -> mixed (kx, y)
-//             MA[y][kx][f]  f = g1,h1,g2,h2 (+ q1,q2,t when velocity-gradient statistics are due)
+//             MA[kx][group][y][W]: the fields f = g1,h1,g2,h2 (| q1,q2,t,0 when velocity-gradient
+//             statistics are due) in records of W = 4 fields, so that a warp's store of one
+//             sub-pass covers 32 consecutive y and the x pass gathers whole 32-byte sectors
 //             g = IFFT_y(u^), h = IFFT_y(i ky u^), q = IFFT_y(ky^2 u^), t = IFFT_y(lap(theta)^)
 //   B  xpass: per y row, three (five) packed complex inverse x transforms give u, du/dx, du/dy
 //             (and lap u, lap theta) in registers; the advective product
 //             N_i = -(u1 d1 u_i + u2 d2 u_i) is formed there and handed, still in registers,
-//             to one packed forward x transform.  Output MB[kx][y][c].
+//             to one packed forward x transform.  Output MB[y/2][kx][y%2][c]: a warp's store
+//             covers consecutive kx of its row, and the y pass gathers whole 32-byte records of
+//             two rows.
 //   C  yfwd : per kx column, forward y transforms, 1/N normalisation, truncation (= the
 //             spherical 2/3 dealias, tool.F90:175-194), viscous term -nu k^2 u^, dilatational
 //             projection (tool.F90:219-243) and the time-integrator combination.
@@ -40,6 +44,20 @@ template <typename T> struct EptOf { static constexpr int v = sizeof(T) == 8 ? B
 #ifndef BASTR_EPT_YFWD_F32
 #define BASTR_EPT_YFWD_F32 8
 #endif
+#ifndef BASTR_EPT_YINV_F32
+#define BASTR_EPT_YINV_F32 16
+#endif
+#ifndef BASTR_MINB_YINV
+#define BASTR_MINB_YINV 0
+#endif
+#ifndef BASTR_XPASS_ROWS
+#define BASTR_XPASS_ROWS 0
+#endif
+#ifndef BASTR_EPT_XPASS_F32
+#define BASTR_EPT_XPASS_F32 16
+#endif
+// Blocks per SM asked of the register allocator: two once an FP32 block has 256 threads.
+template <typename T, int NT> constexpr int minb_for() { return sizeof(T) == 4 && NT >= 256 ? 2 : BASTR_MINB_2D; }
 template <int N, int EPT> constexpr int ept_fit() { return N < EPT ? N : EPT; }
 // Lines handled by one block: at least 128 threads per block.
 template <int NTR> constexpr int groups_per_block() { return NTR >= 128 ? 1 : 128 / NTR; }
@@ -64,23 +82,24 @@ template <typename T, typename TIN, int NY, int SET> struct YInv2D {
     static constexpr int F0 = SET == YI_VG ? 4 : 0;                          // offset in MA
     static constexpr int UG = 2;                                             // units per sub-pass
     static constexpr int NG = (F + UG - 1) / UG;
-    static constexpr int EPT = ept_fit<NY, EptOf<T>::v>();
+    static constexpr int EPT = ept_fit<NY, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_YINV_F32>();
     using FFT = RegFFT<T, NY, EPT, UG, true>;
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
-    static constexpr int MINB = BASTR_MINB_2D;
+    static constexpr int MINB = (BASTR_MINB_YINV > 0 && sizeof(T) == 4) ? BASTR_MINB_YINV : minb_for<T, NT>();
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
     // staging of G columns of KY modes x 2 components, sized at run time
     __host__ __device__ static size_t stage_bytes(int KY) {
         return ((size_t)G * KY * 2 * sizeof(cplx<TIN>) + 15) & ~(size_t)15;
     }
-    static size_t smem(int KY) { return stage_bytes(KY) + XCH; }
+    static constexpr size_t TWB = tw_smem_bytes<T, NY>();
+    static size_t smem(int KY) { return stage_bytes(KY) + XCH + TWB; }
 };
 
 template <typename T, typename TIN, int NY, int SET>
 __global__ void __launch_bounds__(YInv2D<T, TIN, NY, SET>::NT, YInv2D<T, TIN, NY, SET>::MINB)
 k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Geo g,
-         const cplx<T>* __restrict__ tw) {
+         const cplx<T>* tw) {
     using P = YInv2D<T, TIN, NY, SET>;
     using FFT = typename P::FFT;
     constexpr int EPT = P::EPT, UG = P::UG, F = P::F, G = P::G;
@@ -89,6 +108,7 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
     const int K = g.K, KY = g.KY;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY)) + gi * FFT::SMEM_ELEMS;
+    tw = stage_twiddles<T, NY>(reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY) + P::XCH), tw);
     const int nitems = (K + G - 1) / G;
     const int colbytes = KY * 2 * (int)sizeof(cplx<TIN>);
     auto issue = [&](int item) {
@@ -145,12 +165,14 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
             }
             FFT::run(v, sm, tw, t);
             if (valid) {
+                // record width W = min(4, ftot) fields: MA[kx][group][y][W]
+                const int W = ftot < 4 ? ftot : 4;
+                const int f0 = P::F0 + grp * UG;
+                cplx<T>* dst = MA + ((size_t)kx * (ftot / W) + f0 / W) * NY * W + (f0 % W);
 #pragma unroll
                 for (int e = 0; e < EPT; ++e) {
                     const int y = FFT::out_pos(t, e);
-                    cplx<T>* dst = MA + ((size_t)y * K + kx) * ftot + P::F0 + grp * UG;
-                    if (grp * UG + 1 < F) st2<T>(dst, v[e], v[EPT + e]);
-                    else dst[0] = v[e];
+                    st2<T>(dst + (size_t)y * W, v[e], grp * UG + 1 < F ? v[EPT + e] : mk<T>(0, 0));
                 }
             }
         }
@@ -166,23 +188,28 @@ enum XMode : int { XM_RHS = 1, XM_RHS_VG = 2, XM_TO_PHYS = 3, XM_FROM_PHYS = 4 }
 template <typename T, int NX, int MODE> struct XPass2D {
     static constexpr int ZU = MODE == XM_RHS ? 3 : MODE == XM_RHS_VG ? 5 : 1;   // units per row
     static constexpr int FIN = MODE == XM_RHS ? 4 : MODE == XM_RHS_VG ? 8 : MODE == XM_TO_PHYS ? 2 : 0;
-    static constexpr int EPT = ept_fit<NX, EptOf<T>::v>();
+    static constexpr int EPT = ept_fit<NX, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_XPASS_F32>();
     // at most three units share one shared-memory exchange; more run as a second transform
     static constexpr int ZA = ZU > 3 ? 3 : ZU, ZB = ZU - ZA;
     using IFFT = RegFFT<T, NX, EPT, ZA, true>;
     using IFFTB = RegFFT<T, NX, EPT, (ZB > 0 ? ZB : 1), true>;
     using FFFT = RegFFT<T, NX, EPT, 1, false>;
     static constexpr int NTR = IFFT::NTR;
-    static constexpr int G = groups_per_block<NTR>();
+    // rows per block: enough for 128 threads, and BASTR_XPASS_ROWS rows so that the gathered
+    // (kx, pair) pieces of consecutive rows fill whole 32-byte sectors
+    static constexpr int G0 = groups_per_block<NTR>();
+    static constexpr int SR = BASTR_XPASS_ROWS ? 32 / (2 * (int)sizeof(cplx<T>)) : 1;
+    static constexpr int G = (MODE != XM_FROM_PHYS && G0 < SR) ? SR : G0;
     static constexpr int NT = G * NTR;
-    static constexpr int MINB = BASTR_MINB_2D;
+    static constexpr int MINB = G > G0 ? 1 : minb_for<T, NT>();
     static constexpr int KMAX = NX / 3;
     // one staged group: G rows of K*FIN mixed values, or G rows of 2 physical components
     static constexpr size_t STAGE = MODE == XM_FROM_PHYS ? (size_t)G * 2 * NX * sizeof(double)
                                                           : (size_t)G * KMAX * FIN * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
-    static constexpr size_t SMEM = STAGE + XCHR;
+    static constexpr size_t TWB = tw_smem_bytes<T, NX>();
+    static constexpr size_t SMEM = STAGE + XCHR + TWB;
 };
 
 // Packs the half-spectrum values A, B of wavenumber k (0 <= k < K) for one position of a
@@ -198,7 +225,7 @@ template <typename T, int NX, int MODE>
 __global__ void __launch_bounds__(XPass2D<T, NX, MODE>::NT, XPass2D<T, NX, MODE>::MINB)
 k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
           const double* __restrict__ phys_in, double* __restrict__ phys_out,
-          double* __restrict__ vg_part, Geo g, const cplx<T>* __restrict__ tw) {
+          double* __restrict__ vg_part, Geo g, const cplx<T>* tw) {
     using P = XPass2D<T, NX, MODE>;
     using IFFT = typename P::IFFT;
     using FFFT = typename P::FFFT;
@@ -207,6 +234,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
     unsigned char* stg = smraw;
     const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * IFFT::SMEM_ELEMS;
+    tw = stage_twiddles<T, NX>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
     const int K = g.K, NY = g.ny;
     const int nitems = (NY + G - 1) / G;
     auto issue = [&](int item) {
@@ -217,7 +245,19 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
             stage_line(d, phys_in + (size_t)y0 * NX, nrow * NX * 8);
             stage_line(d + G * NX, phys_in + (size_t)NY * NX + (size_t)y0 * NX, nrow * NX * 8);
         } else {
-            stage_line(stg, MA + (size_t)y0 * K * ftot, nrow * K * ftot * (int)sizeof(cplx<T>));
+            // rows y0.. of every (kx, pair) -> staging [kx][pair][row][2]
+            constexpr int W = FIN < 4 ? FIN : 4;
+            constexpr int NPIN = FIN / W, C16 = W * (int)sizeof(cplx<T>) / 16;
+            const int total = K * NPIN * G * C16;
+            for (int i = threadIdx.x; i < total; i += NT) {
+                const int q = i / C16, c = i - q * C16;
+                const int kp = q / G, r = q - kp * G;
+                if (r < nrow) {
+                    const int k = kp / NPIN, pr = kp - k * NPIN;
+                    cp_async16(stg + (size_t)i * 16,
+                               MA + (((size_t)k * (ftot / W) + pr) * NY + y0 + r) * W + c * (16 / (int)sizeof(cplx<T>)));
+                }
+            }
         }
         cp_async_commit();
     };
@@ -239,7 +279,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 v[e] = valid ? mk<T>((T)row[x], (T)row[G * NX + x]) : mk<T>(0, 0);
             }
         } else {
-            const cplx<T>* row = reinterpret_cast<const cplx<T>*>(stg) + (size_t)gi * K * FIN;
+            constexpr int W = FIN < 4 ? FIN : 4;
+            const cplx<T>* row = reinterpret_cast<const cplx<T>*>(stg) + (size_t)gi * W;
 #pragma unroll
             for (int e = 0; e < EPT; ++e) {
                 const int p = IFFT::in_pos(t, e);
@@ -248,8 +289,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
 #pragma unroll
                 for (int u = 0; u < ZU; ++u) v[u * EPT + e] = mk<T>(0, 0);
                 if (valid && (lo || hi)) {
-                    const cplx<T>* src0 = row + (size_t)k * FIN;
-                    auto src = [&](int f) { return src0[f]; };
+                    const cplx<T>* src0 = row + (size_t)k * (FIN / W) * G * W;
+                    auto src = [&](int f) { return src0[(f / W) * G * W + (f % W)]; };
                     const bool z0 = p == 0;
                     const cplx<T> g1 = src(0);
                     if constexpr (MODE == XM_TO_PHYS) {
@@ -331,7 +372,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 for (int k = t; k < K; k += NTR) {
                     const cplx<T> Z = sm[pidx(k)];
                     const cplx<T> Zc = cconj<T>(sm[pidx(k == 0 ? 0 : NX - k)]);
-                    st2<T>(MB + ((size_t)k * NY + y) * 2, cscale<T>(cadd<T>(Z, Zc), (T)0.5),
+                    st2<T>(MB + (((size_t)(y >> 1) * K + k) * 2 + (y & 1)) * 2, cscale<T>(cadd<T>(Z, Zc), (T)0.5),
                            cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5));
                 }
             }
@@ -363,13 +404,14 @@ template <typename T, int NY> struct YFwd2D {
     static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
-    static constexpr size_t SMEM = STAGE + XCHR;
+    static constexpr size_t TWB = tw_smem_bytes<T, NY>();
+    static constexpr size_t SMEM = STAGE + XCHR + TWB;
 };
 
 template <typename T, int NY, int EPI>
 __global__ void __launch_bounds__(YFwd2D<T, NY>::NT, YFwd2D<T, NY>::MINB)
 k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
-         const cplx<T>* __restrict__ tw) {
+         const cplx<T>* tw) {
     using P = YFwd2D<T, NY>;
     using FFT = typename P::FFT;
     constexpr int EPT = P::EPT, NT = P::NT, G = P::G;
@@ -377,12 +419,22 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
     cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
+    tw = stage_twiddles<T, NY>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
     const int K = g.K, KY = g.KY;
     const int nitems = (K + G - 1) / G;
+    // columns kx0.. of every row (records of two rows in MB) -> staging [col][y][c]
     auto issue = [&](int item) {
         const int kx0 = item * G;
         const int ncol = min(G, K - kx0);
-        stage_line(stg, MB + (size_t)kx0 * NY * 2, ncol * NY * 2 * (int)sizeof(cplx<T>));
+        constexpr int C16 = 2 * (int)sizeof(cplx<T>) / 16;
+        const int total = NY * G * C16;
+        for (int i = threadIdx.x; i < total; i += NT) {
+            const int q = i / C16, c = i - q * C16;
+            const int col = q % G, y = q / G;
+            if (col < ncol)
+                cp_async16(reinterpret_cast<unsigned char*>(stg) + ((size_t)(col * NY + y) * 2 * sizeof(cplx<T>) + c * 16),
+                           MB + (((size_t)(y >> 1) * K + kx0 + col) * 2 + (y & 1)) * 2 + c * (16 / (int)sizeof(cplx<T>)));
+        }
         cp_async_commit();
     };
     const double inv_n = g.inv_n;
@@ -408,24 +460,35 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
         FFT::run(v, sm, tw, t);
         if (valid) {
             const double w = kx == 0 ? 1.0 : 2.0;
+            const bool from_u0 = input_is_u0 != 0;
+            constexpr int CH = EPT < EpiChunk<T, 2>::v ? EPT : EpiChunk<T, 2>::v;
 #pragma unroll
-            for (int e = 0; e < EPT; ++e) {
-                const int p = FFT::out_pos(t, e);
-                const int kyi = pos_trunc(p, K, KY, NY);
-                if (kyi < 0) continue;
-                const int ky = trunc_k(kyi, K, KY);
-                const size_t o = ((size_t)kx * KY + kyi) * 2;
-                const long long m2i = (long long)kx * kx + (long long)ky * ky;
-                double2 vv[2];
-                if (m2i < K2) {   // spherical 2/3 rule, tool.F90:185-193
-                    vv[0] = dscale(cvt<cplx<T>, double2>(v[e]), inv_n);
-                    vv[1] = dscale(cvt<cplx<T>, double2>(v[EPT + e]), inv_n);
-                } else {
-                    vv[0] = make_double2(0, 0);
-                    vv[1] = make_double2(0, 0);
+            for (int e0 = 0; e0 < EPT; e0 += CH) {
+                EpiIn<T, 2> in[CH];
+#pragma unroll
+                for (int j = 0; j < CH; ++j) {
+                    const int kyi = pos_trunc(FFT::out_pos(t, e0 + j), K, KY, NY);
+                    if (kyi >= 0) epi_load<T, 2, EPI>(in[j], ((size_t)kx * KY + kyi) * 2, 1, io, from_u0);
                 }
-                const double kv[2] = {(double)kx, (double)ky};
-                rk_epilogue<T, 2, EPI>(vv, kv, (double)m2i, o, 1, io, input_is_u0 != 0, g, w, en);
+#pragma unroll
+                for (int j = 0; j < CH; ++j) {
+                    const int e = e0 + j;
+                    const int kyi = pos_trunc(FFT::out_pos(t, e), K, KY, NY);
+                    if (kyi < 0) continue;
+                    const int ky = trunc_k(kyi, K, KY);
+                    const size_t o = ((size_t)kx * KY + kyi) * 2;
+                    const long long m2i = (long long)kx * kx + (long long)ky * ky;
+                    double2 vv[2];
+                    if (m2i < K2) {   // spherical 2/3 rule, tool.F90:185-193
+                        vv[0] = dscale(cvt<cplx<T>, double2>(v[e]), inv_n);
+                        vv[1] = dscale(cvt<cplx<T>, double2>(v[EPT + e]), inv_n);
+                    } else {
+                        vv[0] = make_double2(0, 0);
+                        vv[1] = make_double2(0, 0);
+                    }
+                    const double kv[2] = {(double)kx, (double)ky};
+                    rk_apply<T, 2, EPI>(vv, kv, (double)m2i, in[j], o, 1, io, from_u0, g, w, en);
+                }
             }
         }
     }

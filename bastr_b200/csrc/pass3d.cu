@@ -603,23 +603,35 @@ k3d_zfwd(const cplx<T>* __restrict__ MD, StageIO<T> io, int input_is_u0, Geo g, 
         if (valid) {
             const int ky = trunc_k(kyi, K, KY);
             const double w = kx == 0 ? 1.0 : 2.0;
+            const bool from_u0 = input_is_u0 != 0;
+            constexpr int CH = EPT < EpiChunk<T, 3>::v ? EPT : EpiChunk<T, 3>::v;
 #pragma unroll
-            for (int e = 0; e < EPT; ++e) {
-                const int kzi = pos_trunc(FFT::out_pos(t, e), K, KZ, NZ);
-                if (kzi < 0) continue;
-                const int kz = trunc_k(kzi, K, KZ);
-                const size_t o = (size_t)l * KZ + kzi;   // component planes g.ps apart
-                const long long m2i = (long long)kx * kx + (long long)ky * ky + (long long)kz * kz;
-                double2 vv[3];
-                if (m2i < K2) {   // spherical 2/3 rule, tool.F90:206-214
+            for (int e0 = 0; e0 < EPT; e0 += CH) {
+                EpiIn<T, 3> in[CH];
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) vv[c] = dscale(cvt<cplx<T>, double2>(v[c * EPT + e]), inv_n);
-                } else {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) vv[c] = make_double2(0, 0);
+                for (int j = 0; j < CH; ++j) {
+                    const int kzi = pos_trunc(FFT::out_pos(t, e0 + j), K, KZ, NZ);
+                    if (kzi >= 0) epi_load<T, 3, EPI>(in[j], (size_t)l * KZ + kzi, (size_t)g.ps, io, from_u0);
                 }
-                const double kv[3] = {(double)kx, (double)ky, (double)kz};
-                rk_epilogue<T, 3, EPI>(vv, kv, (double)m2i, o, (size_t)g.ps, io, input_is_u0 != 0, g, w, en);
+#pragma unroll
+                for (int j = 0; j < CH; ++j) {
+                    const int e = e0 + j;
+                    const int kzi = pos_trunc(FFT::out_pos(t, e), K, KZ, NZ);
+                    if (kzi < 0) continue;
+                    const int kz = trunc_k(kzi, K, KZ);
+                    const size_t o = (size_t)l * KZ + kzi;   // component planes g.ps apart
+                    const long long m2i = (long long)kx * kx + (long long)ky * ky + (long long)kz * kz;
+                    double2 vv[3];
+                    if (m2i < K2) {   // spherical 2/3 rule, tool.F90:206-214
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) vv[c] = dscale(cvt<cplx<T>, double2>(v[c * EPT + e]), inv_n);
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) vv[c] = make_double2(0, 0);
+                    }
+                    const double kv[3] = {(double)kx, (double)ky, (double)kz};
+                    rk_apply<T, 3, EPI>(vv, kv, (double)m2i, in[j], o, (size_t)g.ps, io, from_u0, g, w, en);
+                }
             }
         }
     }

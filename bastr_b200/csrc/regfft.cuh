@@ -140,4 +140,24 @@ struct RegFFT {
     }
 };
 
+// Twiddles a length-N RegFFT reads: w^m for m < N/2 (the largest index any stage forms is
+// R/2 * k * N/(PS*R) < N/2).  Kernels copy them into shared memory once per block.
+#ifndef BASTR_TW_SMEM
+#define BASTR_TW_SMEM 1
+#endif
+template <typename T, int N> constexpr size_t tw_smem_bytes() {
+    return BASTR_TW_SMEM ? (size_t)(N / 2) * sizeof(cplx<T>) : 0;
+}
+// Copies the table into `dst` (tw_smem_bytes<T, N>() of shared memory) and returns the table
+// the transforms should read; the caller's next __syncthreads() publishes the copy.
+template <typename T, int N>
+__device__ __forceinline__ const cplx<T>* stage_twiddles(cplx<T>* dst, const cplx<T>* __restrict__ src) {
+    if constexpr (BASTR_TW_SMEM) {
+        for (int i = threadIdx.x; i < N / 2; i += blockDim.x) dst[i] = src[i];
+        return dst;
+    } else {
+        return src;
+    }
+}
+
 }  // namespace bastr

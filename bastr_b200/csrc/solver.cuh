@@ -122,15 +122,37 @@ __device__ __forceinline__ double2 ld_stage(const StageIO<T>& io, size_t o, bool
 __device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 dscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 
+// State values one mode's epilogue reads: the FP64 state a = u0, the stage input s (us; equal to
+// a when the stage starts from u0) and the RK accumulator p.  Loading them for several modes
+// before any store lets those loads overlap instead of paying one memory latency per mode.
+template <typename T, int D> struct EpiIn {
+    double2 a[D];
+    cplx<T> s[D];
+    cplx<T> p[D];
+};
+
+template <typename T, int D, int EPI>
+__device__ __forceinline__ void epi_load(EpiIn<T, D>& in, size_t o, size_t cst, const StageIO<T>& io,
+                                         bool from_u0) {
+    if constexpr (EPI != EPI_STORE) {
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            in.a[c] = io.u0[o + c * cst];
+            if (!from_u0) in.s[c] = io.us[o + c * cst];
+            if constexpr (EPI == EPI_RK2 || EPI == EPI_RK3) in.p[c] = io.acc[o + c * cst];
+        }
+    }
+}
+
 // Spectral epilogue of one mode (compute_ut, solution.F90:841-861 / 903-926, and the time
 // integrators, solution.F90:172-301).  v[c] holds the dealiased, 1/N-normalised transform of
-// the advective product; k[c] the wavenumbers, m2 = |k|^2; o the state offset of component 0;
-// cst the stride between components; w the Hermitian weight of the mode (1 on kx = 0, else 2);
-// en accumulates w*|u0_new|^2.
+// the advective product; k[c] the wavenumbers, m2 = |k|^2; in the mode's state values
+// (epi_load); o the state offset of component 0; cst the stride between components; w the
+// Hermitian weight of the mode (1 on kx = 0, else 2); en accumulates w*|u0_new|^2.
 template <typename T, int D, int EPI>
-__device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double m2, size_t o, size_t cst,
-                                            const StageIO<T>& io, bool from_u0, const Geo& g,
-                                            double w, double& en) {
+__device__ __forceinline__ void rk_apply(double2* v, const double* k, double m2, const EpiIn<T, D>& in,
+                                         size_t o, size_t cst, const StageIO<T>& io, bool from_u0,
+                                         const Geo& g, double w, double& en) {
     if constexpr (EPI == EPI_STORE) {
 #pragma unroll
         for (int c = 0; c < D; ++c) io.u0[o + c * cst] = v[c];
@@ -140,7 +162,7 @@ __device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double 
 #pragma unroll
         for (int c = 0; c < D; ++c) {
             // + nu * FFT(lap u) with lap u^ = -|k|^2 u^
-            const double2 s = ld_stage<T>(io, o + c * cst, from_u0);
+            const double2 s = from_u0 ? in.a[c] : cvt<cplx<T>, double2>(in.s[c]);
             v[c].x += nu * (-(s.x * m2));
             v[c].y += nu * (-(s.y * m2));
         }
@@ -167,17 +189,17 @@ __device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double 
         const double dt2 = 2.0 * dt;
 #pragma unroll
         for (int c = 0; c < D; ++c) {
-            const double2 a = io.u0[o + c * cst];
+            const double2 a = in.a[c];
             if constexpr (EPI == EPI_RK1) {
                 io.acc[o + c * cst] = cvt<double2, cplx<T>>(v[c]);
                 io.us[o + c * cst] = cvt<double2, cplx<T>>(make_double2(a.x + dt * v[c].x / 2.0, a.y + dt * v[c].y / 2.0));
             } else if constexpr (EPI == EPI_RK2) {
-                const double2 p = cvt<cplx<T>, double2>(io.acc[o + c * cst]);
+                const double2 p = cvt<cplx<T>, double2>(in.p[c]);
                 io.us[o + c * cst] = cvt<double2, cplx<T>>(
                     make_double2(a.x - dt * p.x + dt2 * v[c].x, a.y - dt * p.y + dt2 * v[c].y));
                 io.acc[o + c * cst] = cvt<double2, cplx<T>>(make_double2(p.x + 4.0 * v[c].x, p.y + 4.0 * v[c].y));
             } else if constexpr (EPI == EPI_RK3) {
-                const double2 p = cvt<cplx<T>, double2>(io.acc[o + c * cst]);
+                const double2 p = cvt<cplx<T>, double2>(in.p[c]);
                 const double2 n = make_double2(a.x + dt * (p.x + v[c].x) / 6.0, a.y + dt * (p.y + v[c].y) / 6.0);
                 io.u0[o + c * cst] = n;
                 en += w * (n.x * n.x + n.y * n.y);
@@ -192,6 +214,12 @@ __device__ __forceinline__ void rk_epilogue(double2* v, const double* k, double 
         }
     }
 }
+
+// Modes per thread whose state is fetched together before the epilogue math: more overlap
+// against more live registers (measured best: FP32 2D 4, FP64 2D 2, FP32 3D 2, FP64 3D 4).
+template <typename T, int D> struct EpiChunk {
+    static constexpr int v = D == 2 ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 2 : 4);
+};
 
 // Asynchronous 16-byte global -> shared copies (cp.async, bypassing L1), used to stage whole
 // contiguous lines one iteration ahead of the transform that consumes them.
