@@ -58,6 +58,9 @@ struct bastr_handle {
     double* phys = nullptr;    // physical fields for set/get (d * npts)
     double* vg_part = nullptr;
     double* en_part = nullptr;
+    unsigned int* done = nullptr;  // completion tickets of last-block reductions [kTickets]
+    double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
+    bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
     double* shell = nullptr;   // [nshell][4]
     double* rec = nullptr;     // [kChunk][R_COUNT]
     double* shells_dev = nullptr; // [kChunk][2][allkmax+1]
@@ -88,6 +91,9 @@ struct bastr_handle {
 };
 
 namespace {
+
+// Slots of h->done: one per kind of last-block reduction (each stays 0 between launches).
+enum Ticket : int { T_SPECTRA = 0, kTickets = 4 };
 
 int fail(bastr_handle* h, int code, const char* fmt, ...) {
     char buf[512];
@@ -470,33 +476,36 @@ cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out) {
     if (h->n_items > 0) {
         ProfScope ps(h, "k_spectra", (double)h->n_disk * (h->g.d * 16 + 4));
         if (h->g.d == 2)
-            k_spectra_items<2, 256><<<h->n_items, 256, 0, h->stream>>>(h->u0, h->g, h->sp_modes, h->sp_item_lo,
-                                                                       h->sp_item_part);
+            k_spectra_fused<2, 256><<<h->n_items, 256, 0, h->stream>>>(
+                h->u0, h->g, h->pend, h->sp_modes, h->sp_item_lo, h->sp_item_part, h->done + T_SPECTRA, h->sp_shell_item,
+                h->nshell, h->allkmax, rec, shells_out);
         else
-            k_spectra_items<3, 256><<<h->n_items, 256, 0, h->stream>>>(h->u0, h->g, h->sp_modes, h->sp_item_lo,
-                                                                       h->sp_item_part);
+            k_spectra_fused<3, 256><<<h->n_items, 256, 0, h->stream>>>(
+                h->u0, h->g, h->pend, h->sp_modes, h->sp_item_lo, h->sp_item_part, h->done + T_SPECTRA, h->sp_shell_item,
+                h->nshell, h->allkmax, rec, shells_out);
+    } else {
+        ProfScope ps(h, "k_spectra_final", 0);
+        k_spectra_items_final<256><<<1, 256, 0, h->stream>>>(h->sp_item_part, h->sp_shell_item, h->nshell,
+                                                              h->allkmax, rec, shells_out, h->pend);
     }
-    ProfScope ps(h, "k_spectra_final", (double)h->n_items * 32);
-    k_spectra_items_final<256><<<1, 256, 0, h->stream>>>(h->sp_item_part, h->sp_shell_item, h->nshell,
-                                                          h->allkmax, rec, shells_out);
+    h->scale_pending = false;
     return cudaGetLastError();
 }
 
 cudaError_t launch_forcing(bastr_handle* h, double* rec) {
     const int m = h->p.forcemethod;
     if (m == 0) return cudaSuccess;
-    if (m == 1 || m == 5) {
+    if (m == 1) {
+        ProfScope ps(h, "k_force_linear", (double)h->n_en_blocks * 8);
+        k_force_linear<256><<<1, 256, 0, h->stream>>>(h->en_part, h->n_en_blocks, rec, h->p.target_energy, h->pend);
+        h->scale_pending = true;
+        return cudaGetLastError();
+    }
+    if (m == 5) {
         ProfScope ps(h, "k_sum_partials", (double)h->n_en_blocks * 8);
         k_sum_partials<256><<<1, 256, 0, h->stream>>>(h->en_part, h->n_en_blocks, 1.0, rec, R_ENERGY);
     }
-    if (m == 1) {
-        {
-            ProfScope ps(h, "k_force_linear_factor", 16);
-            k_force_linear_factor<<<1, 32, 0, h->stream>>>(rec, h->p.target_energy);
-        }
-        ProfScope ps(h, "k_scale_state", (double)h->n_state * 32);
-        k_scale_state<<<148 * 4, 256, 0, h->stream>>>(h->u0, h->n_state, rec);
-    } else {
+    {
         const int proj = (m == 5 && h->g.d == 2 && h->p.lprojectd) ? 1 : 0;
         ProfScope ps(h, "k_force_band", 0);
         if (h->g.d == 2)
@@ -538,13 +547,13 @@ cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
 }
 
 int count_launches(bastr_handle* h, bool vg) {
-    int n = 2;                                      // spectra + final
+    int n = 1;                                      // spectra (finished by its last block)
     const int per_rhs = h->g.d == 2 ? 3 : 5;
     const int nrhs = h->p.timemethod == 1 ? 3 : 6;
     n += per_rhs * nrhs;
-    if (vg) n += (h->g.d == 2 ? 1 : 1) + 1;         // extra inverse pass + final reduction
+    if (vg) n += 2;                                 // extra inverse pass + final reduction
     const int m = h->p.forcemethod;
-    if (m == 1) n += 3;
+    if (m == 1) n += 1;
     else if (m == 2) n += 1;
     else if (m == 5) n += 2;
     return n;
@@ -607,7 +616,7 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
 }
 
 void free_all(bastr_handle* h) {
-    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part,
+    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend,
                     h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
                     h->sp_item_part};
     for (void* q : ptrs)
@@ -618,6 +627,18 @@ void free_all(bastr_handle* h) {
     }
     for (cudaEvent_t ev : h->ev_pool) cudaEventDestroy(ev);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+// Applies a linear-forcing scale that the next step's spectra would otherwise apply, so that the
+// state the host reads is the one the reference holds after its forcing.
+cudaError_t flush_pending_scale(bastr_handle* h) {
+    if (!h->scale_pending) return cudaSuccess;
+    k_apply_pending<<<148 * 4, 256, 0, h->stream>>>(h->u0, h->n_state, h->pend);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(h->pend, 0, sizeof(double2), h->stream);
+    h->scale_pending = false;
+    return e;
 }
 
 // Physical <-> truncated spectral state, always in FP64.
@@ -727,6 +748,8 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     dev_alloc(h, &h->acc, h->n_state * cs, st);
     dev_alloc(h, &h->phys, (size_t)d * npts * sizeof(double), st);
     // partial sums: at most one per line group of the passes that produce them
+    dev_alloc(h, &h->done, kTickets * sizeof(unsigned int), st);
+    dev_alloc(h, &h->pend, sizeof(double2), st);
     dev_alloc(h, &h->vg_part, (size_t)std::max(g.ny * g.nz, 1) * 8 * sizeof(double), st);
     dev_alloc(h, &h->en_part, (size_t)std::max(K * g.KY, 1) * sizeof(double), st);
     dev_alloc(h, &h->shell, (size_t)h->nshell * 4 * sizeof(double), st);
@@ -814,6 +837,10 @@ int bastr_set_state(bastr_handle* h, const double* u1, const double* u2, const d
     for (int c = 0; c < h->g.d; ++c)
         CK(cudaMemcpyAsync(h->phys + c * npts, src[c], npts * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CK(to_spectral(h));
+    if (h->scale_pending) {   // a new state replaces the one the scale was meant for
+        CK(cudaMemsetAsync(h->pend, 0, sizeof(double2), h->stream));
+        h->scale_pending = false;
+    }
     CK(cudaStreamSynchronize(h->stream));
     h->have_state = true;
     return BASTR_OK;
@@ -823,6 +850,7 @@ int bastr_get_state(bastr_handle* h, double* u1, double* u2, double* u3) {
     if (!h || !u1 || !u2 || (h->g.d == 3 && !u3)) return fail(h, BASTR_E_INVALID, "null field pointer");
     if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
     CK(cudaSetDevice(h->device));
+    CK(flush_pending_scale(h));
     CK(to_physical(h));
     const size_t npts = (size_t)h->g.nx * h->g.ny * h->g.nz;
     double* dst[3] = {u1, u2, u3};

@@ -1,13 +1,14 @@
 // Per-step diagnostics and forcing on the truncated FP64 state, with deterministic
 // (fixed-order) FP64 reductions: two runs on the same input agree bitwise.
 //
-//  k_spectra        spectra_compute2D/3D (solution.F90:930-1108): one block per shell s,
-//                   enumerating exactly the integer |k|^2 in [s^2-s+1, s^2+s] (the modes with
-//                   nint(|k|) = s, tool.F90:145); Hermitian partners counted by weight 2.
-//  k_spectra_final  shell sums -> Esspe, Edspe, k2Edspe, kMEdspe; copies Es/Ed shells.
+//  k_spectra_fused  spectra_compute2D/3D (solution.F90:930-1108): work items are runs of a
+//                   per-shell list of the stored modes (shell nint(|k|), tool.F90:145; Hermitian
+//                   partners counted by weight 2); the block that finishes last sums the items
+//                   of each shell in fixed order -> Es, Ed shells, Esspe, Edspe, k2Edspe, kMEdspe.
 //  k_velgrad_final  velgrad_calculate2D/3D reductions and derived lengths (solution.F90:1168-1180,
-//                   1268-1280).
+//                   1268-1280) from the x pass's per-block partials.
 //  k_force_*        forcing2D/3D methods 1, 2, 5 (solution.F90:315-378, 483-538, 554-630, 754-812).
+#pragma once
 #include "solver.cuh"
 
 namespace bastr {
@@ -19,9 +20,6 @@ enum RecSlot : int {
     R_FACTOR = 12, R_E = 13, R_ENERGY = 14,
     R_COUNT = 16
 };
-
-// Largest kx range a 2D shell block enumerates (K <= 682 for grids up to 2048).
-constexpr int kSpectraMaxCols = 2048;
 
 __device__ __forceinline__ long long isqrt_floor(long long v) {
     if (v <= 0) return 0;
@@ -38,160 +36,75 @@ __device__ __forceinline__ long long isqrt_ceil(long long v) {
 
 // Adds the contributions of one stored mode (kx >= 0 half) to the shell accumulators.
 template <int D>
-__device__ __forceinline__ void spectra_mode(const double2* __restrict__ U0, const Geo& g, int kx,
-                                             int ky, int kz, double acc[4]) {
+__device__ __forceinline__ void spectra_mode(double2* __restrict__ U0, const Geo& g, int kx,
+                                             int ky, int kz, double acc[4], bool scale = false,
+                                             double f = 1.0) {
     const int K = g.K;
     const int kyi = ky >= 0 ? ky : ky + g.KY;
     const long long m = (long long)kx * kx + (long long)ky * ky + (long long)kz * kz;
     if (m == 0) return;   // kk <= dk/2: us = ud = 0
     const double kk = sqrt((double)m);
+    const double ik = 1.0 / kk;
     const double w = kx == 0 ? 1.0 : 2.0;
-    const double k1 = kx, k2 = ky, k3 = kz;
+    // unit wavevector, one reciprocal per mode
+    const double h1 = kx * ik, h2 = ky * ik, h3 = kz * ik;
     double es, ed;
     if constexpr (D == 2) {
         const size_t o = ((size_t)kx * g.KY + kyi) * 2;
-        const double2 a = U0[o], b = U0[o + 1];
+        double2 a = U0[o], b = U0[o + 1];
+        if (scale) {   // the linear forcing of the previous step, applied here (forcing3D-style u *= f)
+            a = make_double2(f * a.x, f * a.y);
+            b = make_double2(f * b.x, f * b.y);
+            U0[o] = a;
+            U0[o + 1] = b;
+        }
         // usspe = u1 k2/kk - u2 k1/kk ; udspe = u1 k1/kk + u2 k2/kk  (solution.F90:958-959)
-        const double usx = a.x * k2 / kk - b.x * k1 / kk, usy = a.y * k2 / kk - b.y * k1 / kk;
-        const double udx = a.x * k1 / kk + b.x * k2 / kk, udy = a.y * k1 / kk + b.y * k2 / kk;
+        const double usx = a.x * h2 - b.x * h1, usy = a.y * h2 - b.y * h1;
+        const double udx = a.x * h1 + b.x * h2, udy = a.y * h1 + b.y * h2;
         es = (usx * usx + usy * usy) / 2;
         ed = (udx * udx + udy * udy) / 2;
+        (void)h3;
     } else {
         const int kzi = kz >= 0 ? kz : kz + g.KZ;
         const size_t o = ((size_t)kx * g.KY + kyi) * g.KZ + kzi;
-        const double2 a = U0[o], b = U0[o + g.ps], c = U0[o + 2 * g.ps];
+        double2 a = U0[o], b = U0[o + g.ps], c = U0[o + 2 * g.ps];
+        if (scale) {   // the linear forcing of the previous step, applied here (solution.F90:328-331)
+            a = make_double2(f * a.x, f * a.y);
+            b = make_double2(f * b.x, f * b.y);
+            c = make_double2(f * c.x, f * c.y);
+            U0[o] = a;
+            U0[o + g.ps] = b;
+            U0[o + 2 * g.ps] = c;
+        }
         // solution.F90:1047-1053
-        const double udx = a.x * k1 / kk + b.x * k2 / kk + c.x * k3 / kk;
-        const double udy = a.y * k1 / kk + b.y * k2 / kk + c.y * k3 / kk;
-        const double s1x = a.x - udx * k1 / kk, s1y = a.y - udy * k1 / kk;
-        const double s2x = b.x - udx * k2 / kk, s2y = b.y - udy * k2 / kk;
-        const double s3x = c.x - udx * k3 / kk, s3y = c.y - udy * k3 / kk;
+        const double udx = a.x * h1 + b.x * h2 + c.x * h3;
+        const double udy = a.y * h1 + b.y * h2 + c.y * h3;
+        const double s1x = a.x - udx * h1, s1y = a.y - udy * h1;
+        const double s2x = b.x - udx * h2, s2y = b.y - udy * h2;
+        const double s3x = c.x - udx * h3, s3y = c.y - udy * h3;
         es = (s1x * s1x + s1y * s1y) / 2 + (s2x * s2x + s2y * s2y) / 2 + (s3x * s3x + s3y * s3y) / 2;
         ed = (udx * udx + udy * udy) / 2;
     }
     (void)K;
     acc[0] += w * es;
     acc[1] += w * ed;
-    acc[2] += w * (ed * (kk * kk));
-    acc[3] += w * (ed / kk);
+    acc[2] += w * (ed * (double)m);
+    acc[3] += w * (ed * ik);
 }
 
-template <int D, int NT>
-__global__ void __launch_bounds__(NT) k_spectra(const double2* __restrict__ U0, Geo g,
-                                                double* __restrict__ shell /* [SH][4] */) {
-    __shared__ double scratch[4 * NT];
-    const int s = blockIdx.x;
-    const int K = g.K;
-    const long long lo = s == 0 ? 0 : (long long)s * s - s + 1;
-    long long hi = s == 0 ? 0 : (long long)s * s + s;
-    const long long K2m1 = (long long)K * K - 1;   // kept modes have |k|^2 < K^2
-    if (hi > K2m1) hi = K2m1;
-    double acc[4] = {0, 0, 0, 0};
-    if (lo <= hi) {
-        const int kmax = s < K - 1 ? s : K - 1;
-        if constexpr (D == 2) {
-            // Flatten the shell: per kx the modes are ky in [a,b] and [-b,-a] (a > 0) so that
-            // consecutive threads read consecutive ky of one column.
-            __shared__ int off[kSpectraMaxCols + 1];
-            __shared__ int ka[kSpectraMaxCols], kb[kSpectraMaxCols];
-            for (int kx = threadIdx.x; kx <= kmax; kx += NT) {
-                const long long rlo = lo - (long long)kx * kx, rhi = hi - (long long)kx * kx;
-                int a = 0, b = -1;
-                if (rhi >= 0) {
-                    a = (int)isqrt_ceil(rlo);
-                    b = (int)isqrt_floor(rhi);
-                }
-                ka[kx] = a;
-                kb[kx] = b;
-                off[kx + 1] = b >= a ? 2 * (b - a + 1) - (a == 0 ? 1 : 0) : 0;
-            }
-            if (threadIdx.x == 0) off[0] = 0;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                for (int kx = 1; kx <= kmax + 1; ++kx) off[kx] += off[kx - 1];
-            }
-            __syncthreads();
-            const int total = off[kmax + 1];
-            for (int idx = threadIdx.x; idx < total; idx += NT) {
-                int l = 0, r = kmax;   // last kx with off[kx] <= idx
-                while (l < r) {
-                    const int m = (l + r + 1) >> 1;
-                    if (off[m] <= idx) l = m; else r = m - 1;
-                }
-                const int kx = l;
-                const int rr = idx - off[kx];
-                const int a = ka[kx], b = kb[kx];
-                const int npos = b - a + 1;
-                const int ky = rr < npos ? a + rr : -((a == 0 ? 1 : a) + (rr - npos));
-                spectra_mode<2>(U0, g, kx, ky, 0, acc);
-            }
-        } else {
-            const int ny2 = 2 * kmax + 1;
-            const int npair = (kmax + 1) * ny2;
-            for (int e = threadIdx.x; e < npair; e += NT) {
-                const int kx = e / ny2, ky = e - kx * ny2 - kmax;
-                const long long rr = (long long)kx * kx + (long long)ky * ky;
-                const long long rlo = lo - rr, rhi = hi - rr;
-                if (rhi < 0) continue;
-                const int a = (int)isqrt_ceil(rlo), b = (int)isqrt_floor(rhi);
-                for (int kz = a; kz <= b; ++kz) {
-                    spectra_mode<3>(U0, g, kx, ky, kz, acc);
-                    if (kz != 0) spectra_mode<3>(U0, g, kx, ky, -kz, acc);
-                }
-            }
-        }
-    }
-    block_sum<4, NT>(acc, scratch);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) shell[(size_t)s * 4 + i] = acc[i];
-    }
-}
-
-// Shell sums from a precomputed mode list: `modes` holds the state offset (in modes) of every
-// kept mode with 0 < |k|^2 < K^2, grouped by shell nint(|k|) and in increasing offset within a
-// shell; work item i covers modes [item_lo[i], item_lo[i+1]) of one shell.  One block per item
-// writes its four partial sums; consecutive threads read consecutive list entries.
-template <int D, int NT>
-__global__ void __launch_bounds__(NT) k_spectra_items(const double2* __restrict__ U0, Geo g,
-                                                      const int* __restrict__ modes,
-                                                      const int* __restrict__ item_lo,
-                                                      double* __restrict__ item_part /* [items][4] */) {
-    __shared__ double scratch[4 * NT];
-    const int lo = item_lo[blockIdx.x], hi = item_lo[blockIdx.x + 1];
-    double acc[4] = {0, 0, 0, 0};
-    for (int i = lo + threadIdx.x; i < hi; i += NT) {
-        const int m = modes[i];
-        if constexpr (D == 2) {
-            const int kx = m / g.KY, kyi = m - kx * g.KY;
-            spectra_mode<2>(U0, g, kx, trunc_k(kyi, g.K, g.KY), 0, acc);
-        } else {
-            const int kzi = m % g.KZ, r = m / g.KZ;
-            const int kx = r / g.KY, kyi = r - kx * g.KY;
-            spectra_mode<3>(U0, g, kx, trunc_k(kyi, g.K, g.KY), trunc_k(kzi, g.K, g.KZ), acc);
-        }
-    }
-    block_sum<4, NT>(acc, scratch);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) item_part[(size_t)blockIdx.x * 4 + i] = acc[i];
-    }
-}
-
-// Per-shell sums of the work items (items of shell s are shell_item[s] .. shell_item[s+1]-1),
+// Shell sums from the item partials (items of shell s are shell_item[s] .. shell_item[s+1]-1),
 // totals over all shells in fixed order, and the copy of shells 0..allkmax for the spect log.
+// Run by one whole block; reads the partials through L2.
 template <int NT>
-__global__ void __launch_bounds__(NT) k_spectra_items_final(const double* __restrict__ item_part,
-                                                            const int* __restrict__ shell_item, int nshell,
-                                                            int allkmax, double* __restrict__ rec,
-                                                            double* __restrict__ shells_out) {
-    __shared__ double scratch[4 * NT];
+__device__ __forceinline__ void spectra_finish(const double* item_part, const int* __restrict__ shell_item,
+                                               int nshell, int allkmax, double* __restrict__ rec,
+                                               double* __restrict__ shells_out, double* scratch) {
     double acc[4] = {0, 0, 0, 0};
     for (int s = threadIdx.x; s < nshell; s += NT) {
         double sh[4] = {0, 0, 0, 0};
         for (int it = shell_item[s]; it < shell_item[s + 1]; ++it) {
 #pragma unroll
-            for (int i = 0; i < 4; ++i) sh[i] += item_part[(size_t)it * 4 + i];
+            for (int i = 0; i < 4; ++i) sh[i] += __ldcg(item_part + (size_t)it * 4 + i);
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i) acc[i] += sh[i];
@@ -215,43 +128,89 @@ __global__ void __launch_bounds__(NT) k_spectra_items_final(const double* __rest
     }
 }
 
-// Totals over all shells (fixed order) and a copy of shells 0..allkmax for the spect log.
-template <int NT>
-__global__ void __launch_bounds__(NT) k_spectra_final(const double* __restrict__ shell, int nshell,
-                                                      int allkmax, double* __restrict__ rec,
-                                                      double* __restrict__ shells_out /* [2][allkmax+1] */) {
+// One work item per block: its run of list entries, U entries per thread with their index and
+// state loads issued together; then the last block to finish forms the shell sums.
+// pend = (pending, factor): the previous step's linear-forcing scale u *= factor, applied here
+// to every mode that can be non-zero (|k| < K; the others are zero) before its spectra, then
+// cleared by the last block.
+template <int D, int NT>
+__global__ void __launch_bounds__(NT) k_spectra_fused(double2* __restrict__ U0, Geo g, double2* pend,
+                                                      const int* __restrict__ modes,
+                                                      const int* __restrict__ item_lo,
+                                                      double* item_part /* [items][4] */,
+                                                      unsigned int* done, const int* __restrict__ shell_item,
+                                                      int nshell, int allkmax, double* __restrict__ rec,
+                                                      double* __restrict__ shells_out) {
     __shared__ double scratch[4 * NT];
-    double acc[4] = {0, 0, 0, 0};
-    for (int s = threadIdx.x; s < nshell; s += NT) {
+    __shared__ unsigned int flag;
+    constexpr int U = 4;
+    const int lo = item_lo[blockIdx.x], hi = item_lo[blockIdx.x + 1];
+    const double2 pd = pend[0];
+    const bool scale = pd.x != 0.0;
+    if (scale && blockIdx.x == 0 && threadIdx.x == 0) {
+        // the k = 0 mode is in no shell list (it adds nothing to the spectra) but is scaled too
+        const size_t cst = D == 2 ? 1 : (size_t)g.ps;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) acc[i] += shell[(size_t)s * 4 + i];
+        for (int c = 0; c < D; ++c) {
+            const double2 v = U0[c * cst];
+            U0[c * cst] = make_double2(pd.y * v.x, pd.y * v.y);
+        }
+    }
+    double acc[4] = {0, 0, 0, 0};
+    for (int i0 = lo + threadIdx.x; i0 < hi; i0 += U * NT) {
+        int m[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) m[j] = i0 + j * NT < hi ? modes[i0 + j * NT] : -1;
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            if (m[j] < 0) continue;
+            if constexpr (D == 2) {
+                const int kx = m[j] / g.KY, kyi = m[j] - kx * g.KY;
+                spectra_mode<2>(U0, g, kx, trunc_k(kyi, g.K, g.KY), 0, acc, scale, pd.y);
+            } else {
+                const int kzi = m[j] % g.KZ, r = m[j] / g.KZ;
+                const int kx = r / g.KY, kyi = r - kx * g.KY;
+                spectra_mode<3>(U0, g, kx, trunc_k(kyi, g.K, g.KY), trunc_k(kzi, g.K, g.KZ), acc, scale, pd.y);
+            }
+        }
     }
     block_sum<4, NT>(acc, scratch);
     if (threadIdx.x == 0) {
-        rec[R_ES] = acc[0];
-        rec[R_ED] = acc[1];
-        rec[R_K2ED] = acc[2];
-        rec[R_KMED] = acc[3];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) item_part[(size_t)blockIdx.x * 4 + i] = acc[i];
     }
-    if (shells_out) {
-        for (int s = threadIdx.x; s <= allkmax; s += NT) {
-            shells_out[s] = s < nshell ? shell[(size_t)s * 4 + 0] : 0.0;
-            shells_out[allkmax + 1 + s] = s < nshell ? shell[(size_t)s * 4 + 1] : 0.0;
-        }
+    if (!last_block_arrives(done, &flag)) return;
+    spectra_finish<NT>(item_part, shell_item, nshell, allkmax, rec, shells_out, scratch);
+    if (threadIdx.x == 0) {
+        *done = 0;
+        pend[0].x = 0.0;   // every block has read it
     }
 }
 
-// velgrad_calculate2D/3D, solution.F90:1168-1184 / 1268-1284.
+// Shell sums alone (used when no mode survives the truncation: every shell is empty, and a
+// pending scale has nothing to act on).
 template <int NT>
-__global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__ part, int nblk,
-                                                      Geo g, double* __restrict__ rec) {
-    __shared__ double scratch[7 * NT];
+__global__ void __launch_bounds__(NT) k_spectra_items_final(const double* __restrict__ item_part,
+                                                            const int* __restrict__ shell_item, int nshell,
+                                                            int allkmax, double* __restrict__ rec,
+                                                            double* __restrict__ shells_out, double2* pend) {
+    __shared__ double scratch[4 * NT];
+    spectra_finish<NT>(item_part, shell_item, nshell, allkmax, rec, shells_out, scratch);
+    if (threadIdx.x == 0) pend[0].x = 0.0;
+}
+
+// velgrad_calculate2D/3D, solution.F90:1168-1184 / 1268-1284: sums of the nblk per-block
+// partials [7 sums, max|theta|] in fixed order and the derived statistics.  Run by one whole
+// block (scratch: 7*NT doubles); reads the partials through L2.
+template <int NT>
+__device__ __forceinline__ void velgrad_finish(const double* part, int nblk, const Geo& g,
+                                               double* __restrict__ rec, double* scratch) {
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     double dm = 0.0;   // largest |theta| over the grid
     for (int b = threadIdx.x; b < nblk; b += NT) {
 #pragma unroll
-        for (int i = 0; i < 7; ++i) acc[i] += part[(size_t)b * 8 + i];
-        dm = fmax(dm, part[(size_t)b * 8 + 7]);
+        for (int i = 0; i < 7; ++i) acc[i] += __ldcg(part + (size_t)b * 8 + i);
+        dm = fmax(dm, __ldcg(part + (size_t)b * 8 + 7));
     }
     block_sum<7, NT>(acc, scratch);
     dm = -block_min<NT>(-dm, scratch);
@@ -285,6 +244,13 @@ __global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__
     }
 }
 
+template <int NT>
+__global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__ part, int nblk,
+                                                      Geo g, double* __restrict__ rec) {
+    __shared__ double scratch[7 * NT];
+    velgrad_finish<NT>(part, nblk, g, rec, scratch);
+}
+
 // Sum of per-block partials in fixed order -> rec[slot] (scaled).
 template <int NT>
 __global__ void __launch_bounds__(NT) k_sum_partials(const double* __restrict__ part, int n, double scale,
@@ -296,18 +262,31 @@ __global__ void __launch_bounds__(NT) k_sum_partials(const double* __restrict__ 
     if (threadIdx.x == 0) rec[slot] = acc[0] * scale;
 }
 
-// Linear forcing, method 1: factor = sqrt(target / mean(|u|^2/2)).  rec[R_ENERGY] holds
-// sum_k w|u^|^2 = mean(|u|^2) (Parseval with the 1/N forward normalisation).
-__global__ void k_force_linear_factor(double* __restrict__ rec, double target) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        const double energy = rec[R_ENERGY] / 2.0;
-        rec[R_FACTOR] = sqrt(target / energy);
+// Linear forcing, method 1 (solution.F90:315-378): the energy partials of the last stage sum in
+// fixed order to sum_k w|u^|^2 = mean(|u|^2) (Parseval with the 1/N forward normalisation);
+// factor = sqrt(target / mean(|u|^2/2)).  The scale u *= factor itself is left pending: the
+// next step's spectra kernel (or k_apply_pending) applies it.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_force_linear(const double* __restrict__ part, int n,
+                                                     double* __restrict__ rec, double target, double2* pend) {
+    __shared__ double scratch[NT];
+    double acc[1] = {0};
+    for (int b = threadIdx.x; b < n; b += NT) acc[0] += part[b];
+    block_sum<1, NT>(acc, scratch);
+    if (threadIdx.x == 0) {
+        rec[R_ENERGY] = acc[0];
+        const double factor = sqrt(target / (acc[0] / 2.0));
+        rec[R_FACTOR] = factor;
         rec[R_E] = 0.0 / 0.0;
+        pend[0] = make_double2(1.0, factor);
     }
 }
 
-__global__ void k_scale_state(double2* __restrict__ U0, size_t n, const double* __restrict__ rec) {
-    const double f = rec[R_FACTOR];
+// Applies a pending linear-forcing scale to the whole state (before the host reads it).
+__global__ void k_apply_pending(double2* __restrict__ U0, size_t n, const double2* __restrict__ pend) {
+    const double2 pd = pend[0];
+    if (pd.x == 0.0) return;
+    const double f = pd.y;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         double2 v = U0[i];
         U0[i] = make_double2(f * v.x, f * v.y);

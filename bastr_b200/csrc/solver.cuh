@@ -96,6 +96,22 @@ __device__ __forceinline__ double block_min(double v, double* scratch) {
     return r;
 }
 
+// Completion ticket of a reduction whose per-block partials are finished by one block: every
+// block calls this after writing its partials (thread 0 wrote them); it returns true in the one
+// block that arrives last, which then sees all partials and must reset *done to 0 when it is
+// through.  `flag` is one shared word.  No block waits for another.
+__device__ __forceinline__ bool last_block_arrives(unsigned int* done, unsigned int* flag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        *flag = atomicAdd(done, 1u) == gridDim.x - 1 ? 1u : 0u;
+    }
+    __syncthreads();
+    const bool last = *flag != 0;
+    if (last) __threadfence();
+    return last;
+}
+
 // Epilogue modes of the forward pass that closes a right-hand side evaluation.
 enum EpiMode : int {
     EPI_STORE = 0,   // state <- dealiased spectrum (set_state)
