@@ -17,6 +17,15 @@
 #include <vector>
 
 #include "../../include/bastr_gpu.h"
+#ifndef BASTR_PDL
+#define BASTR_PDL 1
+#endif
+// Returns the launch error from the enclosing cudaError_t function.
+#define LAUNCH(...)                                 \
+    do {                                            \
+        cudaError_t le_ = (__VA_ARGS__);            \
+        if (le_ != cudaSuccess) return le_;         \
+    } while (0)
 #include "diag.cu"
 #include "pass2d.cu"
 #include "pass3d.cu"
@@ -151,6 +160,24 @@ template <typename T> const cplx<T>* twp(const Twiddles& t);
 template <> const cplx<double>* twp<double>(const Twiddles& t) { return t.d64; }
 template <> const cplx<float>* twp<float>(const Twiddles& t) { return t.d32; }
 
+// Launches a kernel of the step on the handle's stream with programmatic dependent launch: it may
+// start while the previous kernel drains, and waits for it on the device (pdl_wait).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(bastr_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                     Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = BASTR_PDL;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // Enables the dynamic shared memory a kernel instance asks for and returns how many of its
 // blocks fit on one SM; both once per (device, kernel).
 std::mutex g_prep_mu;
@@ -226,7 +253,7 @@ cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
         const double K_ = h->g.K;
         ProfScope ps(h, SET == YI_VG ? "k2d_yinv_vg" : "k2d_yinv",
                      K_ * h->g.KY * 2 * sizeof(cplx<TIN>) + (double)h->g.ny * K_ * P::F * sizeof(cplx<T>));
-        k<<<grid, P::NT, smem, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[1]));
+        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[1])));
     });
     return cudaGetLastError();
 }
@@ -245,8 +272,8 @@ cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const 
         const double b = MODE == XM_RHS ? mix * 6 * cs : MODE == XM_RHS_VG ? mix * 9 * cs
                        : MODE == XM_TO_PHYS ? mix * 2 * cs + phys : phys + mix * 2 * cs;
         ProfScope ps(h, MODE == XM_RHS_VG ? "k2d_xpass_vg" : MODE == XM_RHS ? "k2d_xpass" : "k2d_xpass_state", b);
-        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg, h->g,
-                                                twp<T>(h->tw[0]));
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg, h->g,
+                                                twp<T>(h->tw[0])));
     });
     return cudaGetLastError();
 }
@@ -263,7 +290,7 @@ cudaError_t l2_yfwd(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0)
         const double cs = sizeof(cplx<T>);
         ProfScope ps(h, "k2d_yfwd", (double)h->g.K * h->g.ny * 2 * cs +
                                     epi_bytes(EPI, from_u0, (double)h->g.K * h->g.KY * 2, cs));
-        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]));
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1])));
     });
     return cudaGetLastError();
 }
@@ -324,7 +351,7 @@ cudaError_t l3_zinv(bastr_handle* h, const void* S, void* MA, int ftot) {
         const double lines = (double)h->g.K * h->g.KY;
         ProfScope ps(h, SET == ZI_VG ? "k3d_zinv_vg" : "k3d_zinv",
                      lines * h->g.KZ * 3 * sizeof(cplx<TIN>) + lines * h->g.nz * P::F * sizeof(cplx<T>));
-        k<<<grid, P::NT, smem, h->stream>>>((const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[2]));
+        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[2])));
     });
     return cudaGetLastError();
 }
@@ -341,7 +368,7 @@ cudaError_t l3_yinv(bastr_handle* h, const void* MA, void* MB) {
         const double cs = sizeof(cplx<T>);
         ProfScope ps(h, SET == YB_RHS_VG ? "k3d_yinv_vg" : "k3d_yinv",
                      (double)h->g.K * h->g.nz * (h->g.KY * P::FIN + h->g.ny * P::F) * cs);
-        k<<<grid, P::NT, smem, h->stream>>>((const cplx<T>*)MA, (cplx<T>*)MB, h->g, twp<T>(h->tw[1]));
+        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<T>*)MA, (cplx<T>*)MB, h->g, twp<T>(h->tw[1])));
     });
     return cudaGetLastError();
 }
@@ -360,8 +387,8 @@ cudaError_t l3_xpass(bastr_handle* h, const void* MB, void* MC, const double* pi
         const double b = MODE == X3_RHS ? mix * 12 * cs : MODE == X3_RHS_VG ? mix * 16 * cs
                        : MODE == X3_TO_PHYS ? mix * 3 * cs + phys : phys + mix * 3 * cs;
         ProfScope ps(h, MODE == X3_RHS_VG ? "k3d_xpass_vg" : MODE == X3_RHS ? "k3d_xpass" : "k3d_xpass_state", b);
-        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg, h->g,
-                                                twp<T>(h->tw[0]));
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg, h->g,
+                                                twp<T>(h->tw[0])));
     });
     return cudaGetLastError();
 }
@@ -375,7 +402,7 @@ cudaError_t l3_yfwd(bastr_handle* h, const void* MC, void* MD) {
         cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
         if (e != cudaSuccess) return e;
         ProfScope ps(h, "k3d_yfwd", (double)h->g.K * h->g.nz * (h->g.ny + h->g.KY) * 3 * sizeof(cplx<T>));
-        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MC, (cplx<T>*)MD, h->g, twp<T>(h->tw[1]));
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MC, (cplx<T>*)MD, h->g, twp<T>(h->tw[1])));
     });
     return cudaGetLastError();
 }
@@ -391,7 +418,7 @@ cudaError_t l3_zfwd(bastr_handle* h, const void* MD, StageIO<T> io, int from_u0)
         if (io.energy_part) h->n_en_blocks = grid;
         const double cs = sizeof(cplx<T>), lines = (double)h->g.K * h->g.KY;
         ProfScope ps(h, "k3d_zfwd", lines * h->g.nz * 3 * cs + epi_bytes(EPI, from_u0, lines * h->g.KZ * 3, cs));
-        k<<<grid, P::NT, P::SMEM, h->stream>>>((const cplx<T>*)MD, io, from_u0, h->g, twp<T>(h->tw[2]));
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MD, io, from_u0, h->g, twp<T>(h->tw[2])));
     });
     return cudaGetLastError();
 }
@@ -476,17 +503,17 @@ cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out) {
     if (h->n_items > 0) {
         ProfScope ps(h, "k_spectra", (double)h->n_disk * (h->g.d * 16 + 4));
         if (h->g.d == 2)
-            k_spectra_fused<2, 256><<<h->n_items, 256, 0, h->stream>>>(
-                h->u0, h->g, h->pend, h->sp_modes, h->sp_item_lo, h->sp_item_part, h->done + T_SPECTRA, h->sp_shell_item,
-                h->nshell, h->allkmax, rec, shells_out);
+            LAUNCH(launch_k(h, k_spectra_fused<2, 256>, h->n_items, 256, 0, h->u0, h->g, h->pend, h->sp_modes,
+                            h->sp_item_lo, h->sp_item_part, h->done + T_SPECTRA, h->sp_shell_item, h->nshell,
+                            h->allkmax, rec, shells_out));
         else
-            k_spectra_fused<3, 256><<<h->n_items, 256, 0, h->stream>>>(
-                h->u0, h->g, h->pend, h->sp_modes, h->sp_item_lo, h->sp_item_part, h->done + T_SPECTRA, h->sp_shell_item,
-                h->nshell, h->allkmax, rec, shells_out);
+            LAUNCH(launch_k(h, k_spectra_fused<3, 256>, h->n_items, 256, 0, h->u0, h->g, h->pend, h->sp_modes,
+                            h->sp_item_lo, h->sp_item_part, h->done + T_SPECTRA, h->sp_shell_item, h->nshell,
+                            h->allkmax, rec, shells_out));
     } else {
         ProfScope ps(h, "k_spectra_final", 0);
-        k_spectra_items_final<256><<<1, 256, 0, h->stream>>>(h->sp_item_part, h->sp_shell_item, h->nshell,
-                                                              h->allkmax, rec, shells_out, h->pend);
+        LAUNCH(launch_k(h, k_spectra_items_final<256>, 1, 256, 0, h->sp_item_part, h->sp_shell_item, h->nshell,
+                                                              h->allkmax, rec, shells_out, h->pend));
     }
     h->scale_pending = false;
     return cudaGetLastError();
@@ -497,21 +524,21 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec) {
     if (m == 0) return cudaSuccess;
     if (m == 1) {
         ProfScope ps(h, "k_force_linear", (double)h->n_en_blocks * 8);
-        k_force_linear<256><<<1, 256, 0, h->stream>>>(h->en_part, h->n_en_blocks, rec, h->p.target_energy, h->pend);
+        LAUNCH(launch_k(h, k_force_linear<256>, 1, 256, 0, h->en_part, h->n_en_blocks, rec, h->p.target_energy, h->pend));
         h->scale_pending = true;
         return cudaGetLastError();
     }
     if (m == 5) {
         ProfScope ps(h, "k_sum_partials", (double)h->n_en_blocks * 8);
-        k_sum_partials<256><<<1, 256, 0, h->stream>>>(h->en_part, h->n_en_blocks, 1.0, rec, R_ENERGY);
+        LAUNCH(launch_k(h, k_sum_partials<256>, 1, 256, 0, h->en_part, h->n_en_blocks, 1.0, rec, R_ENERGY));
     }
     {
         const int proj = (m == 5 && h->g.d == 2 && h->p.lprojectd) ? 1 : 0;
         ProfScope ps(h, "k_force_band", 0);
         if (h->g.d == 2)
-            k_force_band<2, 256><<<1, 256, 0, h->stream>>>(h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec);
+            LAUNCH(launch_k(h, k_force_band<2, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec));
         else
-            k_force_band<3, 256><<<1, 256, 0, h->stream>>>(h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec);
+            LAUNCH(launch_k(h, k_force_band<3, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec));
     }
     return cudaGetLastError();
 }
@@ -527,7 +554,7 @@ cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
         if (e != cudaSuccess) return e;
         if (vg) {
             ProfScope ps(h, "k_velgrad_final", (double)h->n_vg_blocks * 64);
-            k_velgrad_final<256><<<1, 256, 0, h->stream>>>(h->vg_part, h->n_vg_blocks, h->g, rec);
+            LAUNCH(launch_k(h, k_velgrad_final<256>, 1, 256, 0, h->vg_part, h->n_vg_blocks, h->g, rec));
         }
         e = launch_rhs(h, EPI_RK2, false, false);
         if (e != cudaSuccess) return e;
@@ -539,7 +566,7 @@ cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
             if (e != cudaSuccess) return e;
             if (vg && s == 1) {
                 ProfScope ps(h, "k_velgrad_final", (double)h->n_vg_blocks * 64);
-                k_velgrad_final<256><<<1, 256, 0, h->stream>>>(h->vg_part, h->n_vg_blocks, h->g, rec);
+                LAUNCH(launch_k(h, k_velgrad_final<256>, 1, 256, 0, h->vg_part, h->n_vg_blocks, h->g, rec));
             }
         }
     }

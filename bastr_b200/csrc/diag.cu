@@ -141,6 +141,7 @@ __global__ void __launch_bounds__(NT) k_spectra_fused(double2* __restrict__ U0, 
                                                       unsigned int* done, const int* __restrict__ shell_item,
                                                       int nshell, int allkmax, double* __restrict__ rec,
                                                       double* __restrict__ shells_out) {
+    pdl_wait();
     __shared__ double scratch[4 * NT];
     __shared__ unsigned int flag;
     constexpr int U = 4;
@@ -194,6 +195,7 @@ __global__ void __launch_bounds__(NT) k_spectra_items_final(const double* __rest
                                                             const int* __restrict__ shell_item, int nshell,
                                                             int allkmax, double* __restrict__ rec,
                                                             double* __restrict__ shells_out, double2* pend) {
+    pdl_wait();
     __shared__ double scratch[4 * NT];
     spectra_finish<NT>(item_part, shell_item, nshell, allkmax, rec, shells_out, scratch);
     if (threadIdx.x == 0) pend[0].x = 0.0;
@@ -247,6 +249,7 @@ __device__ __forceinline__ void velgrad_finish(const double* part, int nblk, con
 template <int NT>
 __global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__ part, int nblk,
                                                       Geo g, double* __restrict__ rec) {
+    pdl_wait();
     __shared__ double scratch[7 * NT];
     velgrad_finish<NT>(part, nblk, g, rec, scratch);
 }
@@ -255,6 +258,7 @@ __global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__
 template <int NT>
 __global__ void __launch_bounds__(NT) k_sum_partials(const double* __restrict__ part, int n, double scale,
                                                      double* __restrict__ rec, int slot) {
+    pdl_wait();
     __shared__ double scratch[NT];
     double acc[1] = {0};
     for (int b = threadIdx.x; b < n; b += NT) acc[0] += part[b];
@@ -269,6 +273,7 @@ __global__ void __launch_bounds__(NT) k_sum_partials(const double* __restrict__ 
 template <int NT>
 __global__ void __launch_bounds__(NT) k_force_linear(const double* __restrict__ part, int n,
                                                      double* __restrict__ rec, double target, double2* pend) {
+    pdl_wait();
     __shared__ double scratch[NT];
     double acc[1] = {0};
     for (int b = threadIdx.x; b < n; b += NT) acc[0] += part[b];
@@ -298,6 +303,7 @@ __global__ void k_apply_pending(double2* __restrict__ U0, size_t n, const double
 template <int D, int NT>
 __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo g, int method, int forcek,
                                                    double target, int project2d, double* __restrict__ rec) {
+    pdl_wait();
     __shared__ double scratch[NT];
     const int s = forcek;
     const int K = g.K;

@@ -109,6 +109,7 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
     const int K = g.K, KY = g.KY;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY)) + gi * FFT::SMEM_ELEMS;
     tw = stage_twiddles<T, NY>(reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY) + P::XCH), tw);
+    pdl_wait();
     const int nitems = (K + G - 1) / G;
     const int colbytes = KY * 2 * (int)sizeof(cplx<TIN>);
     auto issue = [&](int item) {
@@ -235,6 +236,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
     const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * IFFT::SMEM_ELEMS;
     tw = stage_twiddles<T, NX>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
+    pdl_wait();
     const int K = g.K, NY = g.ny;
     const int nitems = (NY + G - 1) / G;
     auto issue = [&](int item) {
@@ -420,6 +422,7 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
     tw = stage_twiddles<T, NY>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
+    pdl_wait();
     const int K = g.K, KY = g.KY;
     const int nitems = (K + G - 1) / G;
     // columns kx0.. of every row (records of two rows in MB) -> staging [col][y][c]

@@ -96,6 +96,15 @@ __device__ __forceinline__ double block_min(double v, double* scratch) {
     return r;
 }
 
+// Programmatic dependent launch: the kernels of a step are launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization, so a kernel's blocks are scheduled as the
+// previous kernel's blocks exit, and each kernel waits here for the previous kernel to complete
+// (and its writes to be visible) before it touches any data that kernel wrote or reads.  An
+// explicit early trigger (griddepcontrol.launch_dependents) measured slower: the waiting blocks
+// then hold SM resources the running kernel could use.  Without the launch attribute this is a
+// no-op.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Completion ticket of a reduction whose per-block partials are finished by one block: every
 // block calls this after writing its partials (thread 0 wrote them); it returns true in the one
 // block that arrives last, which then sees all partials and must reset *done to 0 when it is
