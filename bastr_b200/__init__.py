@@ -38,7 +38,10 @@ EXPORTED = [
     "bastr_create", "bastr_destroy", "bastr_set_state", "bastr_get_state", "bastr_set_counters",
     "bastr_get_counters", "bastr_step", "bastr_step_async", "bastr_step_records", "bastr_spectra",
     "bastr_fft", "bastr_set_stream", "bastr_sync", "bastr_info", "bastr_last_error", "bastr_profile",
-    "bastr_spectra_noalloc",
+    "bastr_spectra_noalloc", "bastr_set_plan",
+    "bastr_ensemble_create", "bastr_ensemble_destroy", "bastr_ensemble_size", "bastr_ensemble_set_state",
+    "bastr_ensemble_get_state", "bastr_ensemble_step", "bastr_ensemble_set_plan", "bastr_ensemble_get_plan",
+    "bastr_ensemble_tune", "bastr_ensemble_last_error",
 ]
 BASTR_E_TOO_LARGE = -6
 
@@ -102,6 +105,17 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_last_error.argtypes = [P, C.c_char_p, C.c_int32]
     lib.bastr_profile.argtypes = [P, C.c_int32, C.POINTER(CKernelStat), C.c_int32, C.POINTER(C.c_int32)]
     lib.bastr_spectra_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P, P, P]
+    lib.bastr_set_plan.argtypes = [P, C.c_int32]
+    lib.bastr_ensemble_create.argtypes = [C.POINTER(CParams), C.c_int32, C.POINTER(P)]
+    lib.bastr_ensemble_destroy.argtypes = [P]
+    lib.bastr_ensemble_size.argtypes = [P, C.POINTER(C.c_int32)]
+    lib.bastr_ensemble_set_state.argtypes = [P, C.c_int32, D, D, D]
+    lib.bastr_ensemble_get_state.argtypes = [P, C.c_int32, D, D, D]
+    lib.bastr_ensemble_step.argtypes = [P, C.c_int32, C.POINTER(CStepOut)]
+    lib.bastr_ensemble_set_plan.argtypes = [P, C.c_int32, C.c_int32]
+    lib.bastr_ensemble_get_plan.argtypes = [P, C.POINTER(C.c_int32)]
+    lib.bastr_ensemble_tune.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, D]
+    lib.bastr_ensemble_last_error.argtypes = [P, C.c_char_p, C.c_int32]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -131,6 +145,16 @@ def miucal(temper: float, ref_tem: float) -> float:
     return temper * math.sqrt(temper) * (1.0 + tc) / (temper + tc)
 
 
+def make_cparams(ia: int, ja: int, ka: int = 0, *, ref_tem: float = 273.15, reynolds: float = 5000.0,
+                 deltat: float = 1e-4, kmax: int = 1 << 30, timemethod: int = 1, forcemethod: int = 0,
+                 forcek: int = 5, target_energy: float = 0.075, lprojectd: bool = False,
+                 precision: str = "fp64", device: int = 0, velgrad_every: int = 1) -> CParams:
+    """The ``bastr_params`` of one field (the ``datin/input.dat`` values the hot path reads)."""
+    return CParams(ia, ja, ka, ref_tem, reynolds, deltat, kmax, timemethod, forcemethod, forcek,
+                   target_energy, 1 if lprojectd else 0,
+                   BASTR_FP32 if precision == "fp32" else BASTR_FP64, device, velgrad_every)
+
+
 class BastrGPU:
     """One solver handle on one GPU (see module docstring)."""
 
@@ -140,9 +164,10 @@ class BastrGPU:
                  target_energy: float = 0.075, lprojectd: bool = False,
                  precision: str = "fp64", device: int = 0, velgrad_every: int = 1):
         self.lib = load_library()
-        p = CParams(ia, ja, ka, ref_tem, reynolds, deltat, kmax, timemethod, forcemethod, forcek,
-                    target_energy, 1 if lprojectd else 0,
-                    BASTR_FP32 if precision == "fp32" else BASTR_FP64, device, velgrad_every)
+        p = make_cparams(ia, ja, ka, ref_tem=ref_tem, reynolds=reynolds, deltat=deltat, kmax=kmax,
+                         timemethod=timemethod, forcemethod=forcemethod, forcek=forcek,
+                         target_energy=target_energy, lprojectd=lprojectd, precision=precision,
+                         device=device, velgrad_every=velgrad_every)
         self._p = p
         self.h = C.c_void_p()
         rc = self.lib.bastr_create(C.byref(p), C.byref(self.h))
@@ -240,6 +265,10 @@ class BastrGPU:
     def sync(self):
         self._check(self.lib.bastr_sync(self.h))
 
+    def set_plan(self, share_log2: int):
+        """Persistent grids on 1/2**share_log2 of the resident blocks (0 = all)."""
+        self._check(self.lib.bastr_set_plan(self.h, share_log2))
+
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.bastr_set_stream(self.h, C.c_void_p(stream_ptr)))
 
@@ -266,3 +295,6 @@ class BastrGPU:
         self._check(self.lib.bastr_fft(self.h, a.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
                                        direction))
         return a
+
+
+from .ensemble import BastrEnsemble, ensemble_configs, partition_by_cost  # noqa: E402,F401

@@ -68,6 +68,7 @@ struct bastr_handle {
     double* vg_part = nullptr;
     double* en_part = nullptr;
     unsigned int* done = nullptr;  // completion tickets of last-block reductions [kTickets]
+    int share_log2 = 0;            // plan: persistent grids use 1/2^share_log2 of the resident blocks
     double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
     bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
     double* shell = nullptr;   // [nshell][4]
@@ -212,14 +213,17 @@ template <typename K> cudaError_t prep(K kernel, size_t smem, int nt = 0, int* b
 }
 
 // Grid of a persistent pass: as many blocks as fit on the device, at most one per work item.
-template <typename K> cudaError_t persistent_grid(K kernel, size_t smem, int nt, int nitems, int* grid) {
+// The handle's plan may restrict its persistent grids to 1/2^share of that (an ensemble runs
+// many handles at once, each on a share of the SMs).
+template <typename K> cudaError_t persistent_grid(const bastr_handle* h, K kernel, size_t smem, int nt, int nitems,
+                                                  int* grid) {
     int nb = 1;
     cudaError_t e = prep(kernel, smem, nt, &nb);
     if (e != cudaSuccess) return e;
     int dev = 0;
     cudaGetDevice(&dev);
     const int sms = (dev >= 0 && dev < 64 && g_num_sms[dev] > 0) ? g_num_sms[dev] : 148;
-    *grid = std::max(1, std::min(nitems, nb * sms));
+    *grid = std::max(1, std::min(nitems, (nb * sms) >> h->share_log2));
     return cudaSuccess;
 }
 
@@ -248,7 +252,7 @@ cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
         auto k = k2d_yinv<T, TIN, NN, SET>;
         const size_t smem = P::smem(h->g.KY);
         int grid = 1;
-        cudaError_t e = persistent_grid(k, smem, P::NT, cdiv(h->g.K, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, smem, P::NT, cdiv(h->g.K, P::G), &grid);
         if (e != cudaSuccess) return e;
         const double K_ = h->g.K;
         ProfScope ps(h, SET == YI_VG ? "k2d_yinv_vg" : "k2d_yinv",
@@ -265,7 +269,7 @@ cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const 
         using P = XPass2D<T, NN, MODE>;
         auto k = k2d_xpass<T, NN, MODE>;
         int grid = 1;
-        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.ny, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.ny, P::G), &grid);
         if (e != cudaSuccess) return e;
         if (MODE == XM_RHS_VG) h->n_vg_blocks = grid;
         const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.K, phys = 2.0 * h->g.nx * h->g.ny * 8;
@@ -284,7 +288,7 @@ cudaError_t l2_yfwd(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0)
         using P = YFwd2D<T, NN>;
         auto k = k2d_yfwd<T, NN, EPI>;
         int grid = 1;
-        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K, P::G), &grid);
         if (e != cudaSuccess) return e;
         if (io.energy_part) h->n_en_blocks = grid;
         const double cs = sizeof(cplx<T>);
@@ -346,7 +350,7 @@ cudaError_t l3_zinv(bastr_handle* h, const void* S, void* MA, int ftot) {
         auto k = k3d_zinv<T, TIN, NN, SET>;
         const size_t smem = P::smem(h->g.KZ);
         int grid = 1;
-        cudaError_t e = persistent_grid(k, smem, P::NT, cdiv(h->g.K * h->g.KY, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, smem, P::NT, cdiv(h->g.K * h->g.KY, P::G), &grid);
         if (e != cudaSuccess) return e;
         const double lines = (double)h->g.K * h->g.KY;
         ProfScope ps(h, SET == ZI_VG ? "k3d_zinv_vg" : "k3d_zinv",
@@ -363,7 +367,7 @@ cudaError_t l3_yinv(bastr_handle* h, const void* MA, void* MB) {
         auto k = k3d_yinv<T, NN, SET>;
         const size_t smem = P::smem(h->g.KY);
         int grid = 1;
-        cudaError_t e = persistent_grid(k, smem, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, smem, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
         if (e != cudaSuccess) return e;
         const double cs = sizeof(cplx<T>);
         ProfScope ps(h, SET == YB_RHS_VG ? "k3d_yinv_vg" : "k3d_yinv",
@@ -379,7 +383,7 @@ cudaError_t l3_xpass(bastr_handle* h, const void* MB, void* MC, const double* pi
         using P = XPass3D<T, NN, MODE>;
         auto k = k3d_xpass<T, NN, MODE>;
         int grid = 1;
-        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.ny * h->g.nz, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.ny * h->g.nz, P::G), &grid);
         if (e != cudaSuccess) return e;
         if (MODE == X3_RHS_VG) h->n_vg_blocks = grid;
         const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.nz * h->g.K;
@@ -399,7 +403,7 @@ cudaError_t l3_yfwd(bastr_handle* h, const void* MC, void* MD) {
         using P = YFwd3D<T, NN>;
         auto k = k3d_yfwd<T, NN>;
         int grid = 1;
-        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
         if (e != cudaSuccess) return e;
         ProfScope ps(h, "k3d_yfwd", (double)h->g.K * h->g.nz * (h->g.ny + h->g.KY) * 3 * sizeof(cplx<T>));
         LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MC, (cplx<T>*)MD, h->g, twp<T>(h->tw[1])));
@@ -413,7 +417,7 @@ cudaError_t l3_zfwd(bastr_handle* h, const void* MD, StageIO<T> io, int from_u0)
         using P = ZFwd3D<T, NN>;
         auto k = k3d_zfwd<T, NN, EPI>;
         int grid = 1;
-        cudaError_t e = persistent_grid(k, P::SMEM, P::NT, cdiv(h->g.K * h->g.KY, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K * h->g.KY, P::G), &grid);
         if (e != cudaSuccess) return e;
         if (io.energy_part) h->n_en_blocks = grid;
         const double cs = sizeof(cplx<T>), lines = (double)h->g.K * h->g.KY;
@@ -901,34 +905,13 @@ int bastr_get_counters(bastr_handle* h, int64_t* nstep, double* time) {
     return BASTR_OK;
 }
 
-int bastr_step_async(bastr_handle* h, int32_t nsteps) {
-    if (!h || nsteps < 0) return fail(h, BASTR_E_INVALID, "nsteps");
-    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
-    if (nsteps > kChunk) return fail(h, BASTR_E_INVALID, "bastr_step_async: at most %d steps per call", kChunk);
-    CK(cudaSetDevice(h->device));
-    h->batch_n0 = h->nstep;
-    h->batch_t0 = h->time;
-    for (int i = 0; i < nsteps; ++i) {
-        const int64_t n = h->nstep;
-        const bool vg = h->p.velgrad_every > 0 && (n % h->p.velgrad_every) == 0;
-        CK(launch_step(h, i, vg));
-        h->nstep += 1;
-        h->time = h->time + h->p.deltat;
-    }
-    h->chunk_used = nsteps;
-    return BASTR_OK;
-}
+}  // extern "C"
 
-int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells) {
-    if (!h) return BASTR_E_INVALID;
-    if (nsteps > h->chunk_used) return fail(h, BASTR_E_INVALID, "only %d records available", h->chunk_used);
-    CK(cudaSetDevice(h->device));
-    std::vector<double> rec((size_t)nsteps * R_COUNT);
-    if (nsteps) CK(cudaMemcpyAsync(rec.data(), h->rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    if (shells && nsteps)
-        CK(cudaMemcpyAsync(shells, h->shells_dev, (size_t)nsteps * 2 * (h->allkmax + 1) * sizeof(double),
-                           cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+namespace {
+
+// Per-step records of the last batch (device slots 0..nsteps-1, R_COUNT doubles each) -> the
+// caller's bastr_step_out array, with nstep/time as the reference counts them.
+void decode_records(const bastr_handle* h, const double* rec, int nsteps, bastr_step_out* out) {
     const int64_t n0 = h->batch_n0;
     double t = h->batch_t0;   // times accumulate exactly as the reference's time = time + deltat
     for (int i = 0; i < nsteps; ++i) {
@@ -945,6 +928,56 @@ int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, dou
         }
         t = t + h->p.deltat;
     }
+}
+
+// Launches nsteps steps on the handle's stream into record slots 0..nsteps-1 and advances the
+// host counters.
+cudaError_t launch_batch(bastr_handle* h, int nsteps) {
+    h->batch_n0 = h->nstep;
+    h->batch_t0 = h->time;
+    for (int i = 0; i < nsteps; ++i) {
+        const int64_t n = h->nstep;
+        const bool vg = h->p.velgrad_every > 0 && (n % h->p.velgrad_every) == 0;
+        cudaError_t e = launch_step(h, i, vg);
+        if (e != cudaSuccess) return e;
+        h->nstep += 1;
+        h->time = h->time + h->p.deltat;
+    }
+    h->chunk_used = nsteps;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bastr_set_plan(bastr_handle* h, int32_t share_log2) {
+    if (!h) return BASTR_E_INVALID;
+    if (share_log2 < 0 || share_log2 > 7) return fail(h, BASTR_E_INVALID, "share_log2 must be in [0, 7]");
+    h->share_log2 = share_log2;
+    return BASTR_OK;
+}
+
+int bastr_step_async(bastr_handle* h, int32_t nsteps) {
+    if (!h || nsteps < 0) return fail(h, BASTR_E_INVALID, "nsteps");
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    if (nsteps > kChunk) return fail(h, BASTR_E_INVALID, "bastr_step_async: at most %d steps per call", kChunk);
+    CK(cudaSetDevice(h->device));
+    CK(launch_batch(h, nsteps));
+    return BASTR_OK;
+}
+
+int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells) {
+    if (!h) return BASTR_E_INVALID;
+    if (nsteps > h->chunk_used) return fail(h, BASTR_E_INVALID, "only %d records available", h->chunk_used);
+    CK(cudaSetDevice(h->device));
+    std::vector<double> rec((size_t)nsteps * R_COUNT);
+    if (nsteps) CK(cudaMemcpyAsync(rec.data(), h->rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (shells && nsteps)
+        CK(cudaMemcpyAsync(shells, h->shells_dev, (size_t)nsteps * 2 * (h->allkmax + 1) * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    decode_records(h, rec.data(), nsteps, out);
     return BASTR_OK;
 }
 
@@ -1076,3 +1109,5 @@ int bastr_last_error(bastr_handle* h, char* buf, int32_t n) {
 }
 
 }  // extern "C"
+
+#include "ensemble.cu"

@@ -50,6 +50,12 @@ template <typename T> struct EptOf { static constexpr int v = sizeof(T) == 8 ? B
 #ifndef BASTR_MINB_YINV
 #define BASTR_MINB_YINV 0
 #endif
+#ifndef BASTR_MINB_XPASS
+#define BASTR_MINB_XPASS 0
+#endif
+#ifndef BASTR_XPASS_TW_SMEM
+#define BASTR_XPASS_TW_SMEM 1
+#endif
 #ifndef BASTR_XPASS_ROWS
 #define BASTR_XPASS_ROWS 0
 #endif
@@ -202,14 +208,14 @@ template <typename T, int NX, int MODE> struct XPass2D {
     static constexpr int SR = BASTR_XPASS_ROWS ? 32 / (2 * (int)sizeof(cplx<T>)) : 1;
     static constexpr int G = (MODE != XM_FROM_PHYS && G0 < SR) ? SR : G0;
     static constexpr int NT = G * NTR;
-    static constexpr int MINB = G > G0 ? 1 : minb_for<T, NT>();
+    static constexpr int MINB = G > G0 ? 1 : (BASTR_MINB_XPASS > 0 && sizeof(T) == 4 && MODE == XM_RHS) ? BASTR_MINB_XPASS : minb_for<T, NT>();
     static constexpr int KMAX = NX / 3;
     // one staged group: G rows of K*FIN mixed values, or G rows of 2 physical components
     static constexpr size_t STAGE = MODE == XM_FROM_PHYS ? (size_t)G * 2 * NX * sizeof(double)
                                                           : (size_t)G * KMAX * FIN * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
-    static constexpr size_t TWB = tw_smem_bytes<T, NX>();
+    static constexpr size_t TWB = BASTR_XPASS_TW_SMEM ? tw_smem_bytes<T, NX>() : 0;
     static constexpr size_t SMEM = STAGE + XCHR + TWB;
 };
 
@@ -235,7 +241,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
     unsigned char* stg = smraw;
     const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * IFFT::SMEM_ELEMS;
-    tw = stage_twiddles<T, NX>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
+    if constexpr (P::TWB > 0) tw = stage_twiddles<T, NX>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
     pdl_wait();
     const int K = g.K, NY = g.ny;
     const int nitems = (NY + G - 1) / G;

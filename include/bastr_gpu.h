@@ -155,6 +155,40 @@ BASTR_API int bastr_spectra_noalloc(int32_t ia, int32_t ja, int32_t ka, int32_t 
 /* Copies the message of the last failed call into buf (NUL-terminated); returns its length. */
 BASTR_API int bastr_last_error(bastr_handle* h, char* buf, int32_t n);
 
+
+/* ------------------------------------------------------------------------------------------
+ * Plan of a handle: its persistent grids use 1/2^share_log2 of the blocks that fit on the GPU
+ * (0 = all, the default).  No reference counterpart (execution plan only; results depend on
+ * it only through the order of the per-block partial sums).
+ * ------------------------------------------------------------------------------------------ */
+BASTR_API int bastr_set_plan(bastr_handle* h, int32_t share_log2);
+
+/* ------------------------------------------------------------------------------------------
+ * Batched ensemble: n independent realizations (each with its own bastr_params: grid size,
+ * forcing, precision; one device for all) advanced together.  No reference counterpart: the
+ * reference runs one field per job.  A batch of nsteps (<= 256) steps of every realization is
+ * one CUDA-graph launch whose branches (one per realization) run concurrently.
+ *
+ *   bastr_ensemble_step    out: [n][nsteps] records, realization-major; BASTR_E_NAN if some
+ *                          realization's Es+Ed became NaN (message names it)
+ *   bastr_ensemble_tune    autotuner of the plans (per grid-size class), timing nsteps steps
+ *                          of the graph best of reps, shares 0..max_share_log2; state restored
+ *   bastr_ensemble_set_plan realization i (-1: all)
+ * ------------------------------------------------------------------------------------------ */
+typedef struct bastr_ensemble bastr_ensemble;
+BASTR_API int bastr_ensemble_create(const bastr_params* params, int32_t n, bastr_ensemble** out);
+BASTR_API int bastr_ensemble_destroy(bastr_ensemble* e);
+BASTR_API int bastr_ensemble_size(bastr_ensemble* e, int32_t* n);
+BASTR_API int bastr_ensemble_set_state(bastr_ensemble* e, int32_t i, const double* u1, const double* u2,
+                                       const double* u3);
+BASTR_API int bastr_ensemble_get_state(bastr_ensemble* e, int32_t i, double* u1, double* u2, double* u3);
+BASTR_API int bastr_ensemble_step(bastr_ensemble* e, int32_t nsteps, bastr_step_out* out);
+BASTR_API int bastr_ensemble_set_plan(bastr_ensemble* e, int32_t i, int32_t share_log2);
+BASTR_API int bastr_ensemble_get_plan(bastr_ensemble* e, int32_t* share_log2);
+BASTR_API int bastr_ensemble_tune(bastr_ensemble* e, int32_t nsteps, int32_t reps, int32_t max_share_log2,
+                                  double* best_ms);
+BASTR_API int bastr_ensemble_last_error(bastr_ensemble* e, char* buf, int32_t n);
+
 #ifdef __cplusplus
 }
 #endif
