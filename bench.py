@@ -191,6 +191,47 @@ def kernel_roofline(s, nsteps, peak, peak_kind, wl, prec):
             "share_of_step": round(top["total_ms"] / total, 4)}, shares
 
 
+def ensemble_measure(device, steps=30, tune=True):
+    """The standard ensemble (96 realizations: 32 each at 256^2, 512^2, 1024^2, seeds 0-95, band
+    forcing with forcek in {3..8}, target in [0.05, 0.1], FP32), advanced as one CUDA graph per
+    batch of steps; host wall time around the synchronous ensemble step calls (records read
+    back every batch), and the same realizations stepped one after another through their own
+    handles for comparison."""
+    from bastr_b200 import BastrEnsemble, BastrGPU, ensemble_configs, seeded_field
+    cfgs = ensemble_configs()
+    fields = [seeded_field(c["ia"], c["ja"], 0, k0=c["k0"], seed=c["seed"]) for c in cfgs]
+    out = {"realizations": len(cfgs), "sizes": sorted({c["ia"] for c in cfgs}), "precision": "fp32"}
+    with BastrEnsemble(cfgs, device=device) as ens:
+        for i, u in enumerate(fields):
+            ens.set_state(i, u)
+        if tune:
+            out["tuned_ms_per_step"] = round(ens.tune(nsteps=4, reps=2, max_share_log2=3), 4)
+            out["plans_log2_by_size"] = {str(n): sorted({p for c, p in zip(cfgs, ens.plans()) if c["ia"] == n})
+                                         for n in out["sizes"]}
+        batch = 10
+        ens.step(batch)   # capture of the batch graph + warm-up
+        t0 = time.perf_counter()
+        for _ in range(steps // batch):
+            ens.step(batch)
+        dt = time.perf_counter() - t0
+        steps = (steps // batch) * batch
+    out["ensemble_steps_per_s"] = round(steps / dt, 2)
+    out["realization_steps_per_s"] = round(steps * len(cfgs) / dt, 1)
+    # one realization after another, each through its own handle
+    t_seq = 0.0
+    for c, u in zip(cfgs, fields):
+        with BastrGPU(c["ia"], c["ja"], 0, deltat=c["deltat"], forcemethod=2, forcek=c["forcek"],
+                      target_energy=c["target_energy"], lprojectd=True, precision="fp32", device=device) as s:
+            s.set_state(u)
+            s.step(2)
+            t1 = time.perf_counter()
+            s.step(steps)
+            t_seq += time.perf_counter() - t1
+    out["sequential_realization_steps_per_s"] = round(steps * len(cfgs) / t_seq, 1)
+    out["timing"] = "host wall time around synchronous step calls (records copied to the host each call)"
+    return out
+
+
 def e2e_measure(wl, prec, steps, device):
     """Through the C ABI with host buffers: upload the field from pinned memory, step with the
     per-step records (scalars + shell spectra) read back every step, download the field."""
@@ -320,6 +361,8 @@ def ours(args):
                                                            / (peak * 1e9), 4),
                              "dominant_kernel": vroof})
     e2e = e2e_measure(wl, prec, max(20, min(args.steps, 200)), device) if (rank == 0 and not args.no_e2e) else None
+    ens = (ensemble_measure(device) if (rank == 0 and n_gpus == 1 and not args.no_variants and not args.no_ensemble)
+           else None)
     base = cpu_baseline(wl) if (rank == 0 and n_gpus == 1 and not args.no_cpu) else None
     if dist_ctx:
         dist_ctx.barrier()
@@ -340,7 +383,7 @@ def ours(args):
                    "l2": "no flush: per-step working set and traffic exceed the 126 MB L2"},
         "mpoint_steps_per_s": round(steps_per_s * npts / 1e6, 1),
         "survey_roofline_frac": round(survey_bytes(w, prec) / (ms / args.steps * 1e-3) / (peak * 1e9), 4),
-        "roofline": roof, "kernel_shares": shares, "variants": variants,
+        "roofline": roof, "kernel_shares": shares, "variants": variants, "ensemble": ens,
         "cpu_baseline": base, "e2e": e2e,
         "gpu_launches": int(info["launches_per_step"] * args.steps),
         "clocks": clocks,
@@ -375,6 +418,7 @@ def main():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=HEADLINE[0],
                     help="headline workload (default: the 2048^2 band-forced case)")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default=HEADLINE[1])
