@@ -29,6 +29,7 @@
 #include "diag.cu"
 #include "pass2d.cu"
 #include "pass3d.cu"
+#include "fullfft.cu"
 
 using namespace bastr;
 
@@ -489,10 +490,42 @@ cudaError_t state3d_to_physical(bastr_handle* h) {
     return l3_xpass<double, X3_TO_PHYS>(h, h->mb, nullptr, nullptr, h->phys, nullptr);
 }
 
+// One axis of the full-grid transform on the device array A (complex, [nz][ny][nx]).
+template <bool INV> cudaError_t full_axis(bastr_handle* h, double2* A, int axis, double scale) {
+    const Geo& g = h->g;
+    const int ns[3] = {g.nx, g.ny, g.nz};
+    const long long total = (long long)g.nx * g.ny * g.nz;
+    const int N = ns[axis];
+    const int nlines = (int)(total / N);
+    const long long S = axis == 0 ? 1 : axis == 1 ? g.nx : (long long)g.nx * g.ny;
+    const long long R = axis == 1 ? (long long)g.nx * g.ny : g.nx;
+    SIZE_CASES(N, {
+        using P = FullLine<NN>;
+        auto k = k_full_axis<NN, INV>;
+        int grid = 1;
+        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(nlines, P::G), &grid);
+        if (e != cudaSuccess) return e;
+        ProfScope ps(h, "k_full_axis", (double)total * 32);
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, A, g.nx, S, R, nlines, scale, (const double2*)h->tw[axis].d64));
+    });
+    return cudaGetLastError();
+}
+
+// bastr_fft: host array -> the handle's physical-field buffer (2 or 3 doubles per point, so a
+// complex grid fits) -> one pass per axis -> host.  dir -1: forward, scaled 1/N on its last axis.
 int full_fft(bastr_handle* h, double* array, int dir) {
-    (void)array;
-    (void)dir;
-    return fail(h, BASTR_E_UNSUPPORTED, "bastr_fft is not built yet");
+    const Geo& g = h->g;
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    double2* A = reinterpret_cast<double2*>(h->phys);
+    CK(cudaMemcpyAsync(A, array, n * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    for (int a = 0; a < g.d; ++a) {
+        const double scale = (dir < 0 && a == g.d - 1) ? g.inv_n : 1.0;
+        if (dir < 0) CK(full_axis<false>(h, A, a, scale));
+        else CK(full_axis<true>(h, A, a, scale));
+    }
+    CK(cudaMemcpyAsync(array, A, n * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return BASTR_OK;
 }
 
 // ---------------------------------------------------------------------------------------
