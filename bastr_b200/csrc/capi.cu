@@ -70,6 +70,7 @@ struct bastr_handle {
     double* en_part = nullptr;
     unsigned int* done = nullptr;  // completion tickets of last-block reductions [kTickets]
     int share_log2 = 0;            // plan: persistent grids use 1/2^share_log2 of the resident blocks
+    bool ma_ready = false;         // 2D: MA already holds pass A of the next stage
     double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
     bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
     double* shell = nullptr;   // [nshell][4]
@@ -150,7 +151,7 @@ double epi_bytes(int epi, bool from_u0, double n, double cs) {
     switch (epi) {
         case EPI_STORE: return n * 16;
         case EPI_RK1: return n * 16 + 2 * n * cs;
-        case EPI_RK2: return 3 * n * cs + n * 16 + 2 * n * cs;
+        case EPI_RK2: return 2 * n * cs + n * 16 + 2 * n * cs;
         case EPI_RK3: return 2 * n * cs + n * 16 + n * 16;
         case EPI_CN_MID: return from_u0 ? n * 16 + n * cs : 2 * n * cs + n * 16;
         case EPI_CN_LAST: return n * cs + 2 * n * 16;
@@ -300,13 +301,38 @@ cudaError_t l2_yfwd(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0)
     return cudaGetLastError();
 }
 
-// One right-hand-side evaluation F(u_s) and its combination, 2D.
+template <typename T, int EPI>
+cudaError_t l2_yfwd_inv(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0, void* MA) {
+    SIZE_CASES(h->g.ny, {
+        using P = YFwdInv2D<T, NN>;
+        auto k = k2d_yfwd_inv<T, NN, EPI>;
+        int grid = 1;
+        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K, P::G), &grid);
+        if (e != cudaSuccess) return e;
+        const double cs = sizeof(cplx<T>);
+        ProfScope ps(h, "k2d_yfwd_inv", (double)h->g.K * h->g.ny * 2 * cs +
+                                        epi_bytes(EPI, from_u0, (double)h->g.K * h->g.KY * 2, cs) +
+                                        (double)h->g.ny * h->g.K * 4 * cs);
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]),
+                        (cplx<T>*)MA));
+    });
+    return cudaGetLastError();
+}
+
+#ifndef BASTR_FUSE_Y
+#define BASTR_FUSE_Y 1
+#endif
+
+// One right-hand-side evaluation F(u_s) and its combination, 2D.  Stages after the first find
+// their pass A already done when the previous stage's forward pass handed its stage input on
+// (k2d_yfwd_inv, h->ma_ready).
 template <typename T>
 cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
-    cudaError_t e;
+    cudaError_t e = cudaSuccess;
     const int ftot = vg ? 8 : 4;
     if (from_u0) e = l2_yinv<T, double, YI_RHS>(h, h->u0, h->ma, ftot);
-    else e = l2_yinv<T, T, YI_RHS>(h, h->us, h->ma, ftot);
+    else if (!h->ma_ready || vg) e = l2_yinv<T, T, YI_RHS>(h, h->us, h->ma, ftot);
+    h->ma_ready = false;
     if (e != cudaSuccess) return e;
     if (vg) {
         e = l2_yinv<T, double, YI_VG>(h, h->u0, h->ma, ftot);
@@ -320,6 +346,14 @@ cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
     const bool need_en = (epi == EPI_RK3 || epi == EPI_CN_LAST) &&
                          (h->p.forcemethod == 1 || h->p.forcemethod == 5);
     if (need_en) io.energy_part = h->en_part;
+    if (BASTR_FUSE_Y && (epi == EPI_RK1 || epi == EPI_RK2 || epi == EPI_CN_MID)) {
+        h->ma_ready = true;
+        switch (epi) {
+            case EPI_RK1: return l2_yfwd_inv<T, EPI_RK1>(h, h->mb, io, from_u0, h->ma);
+            case EPI_RK2: return l2_yfwd_inv<T, EPI_RK2>(h, h->mb, io, from_u0, h->ma);
+            case EPI_CN_MID: return l2_yfwd_inv<T, EPI_CN_MID>(h, h->mb, io, from_u0, h->ma);
+        }
+    }
     switch (epi) {
         case EPI_RK1: return l2_yfwd<T, EPI_RK1>(h, h->mb, io, from_u0);
         case EPI_RK2: return l2_yfwd<T, EPI_RK2>(h, h->mb, io, from_u0);
@@ -615,6 +649,7 @@ int count_launches(bastr_handle* h, bool vg) {
     const int per_rhs = h->g.d == 2 ? 3 : 5;
     const int nrhs = h->p.timemethod == 1 ? 3 : 6;
     n += per_rhs * nrhs;
+    if (h->g.d == 2 && BASTR_FUSE_Y) n -= nrhs - 1;  // pass A of every stage but the first is fused
     if (vg) n += 2;                                 // extra inverse pass + final reduction
     const int m = h->p.forcemethod;
     if (m == 1) n += 1;

@@ -50,6 +50,14 @@ template <typename T> struct EptOf { static constexpr int v = sizeof(T) == 8 ? B
 #ifndef BASTR_MINB_YINV
 #define BASTR_MINB_YINV 0
 #endif
+// Modes per thread whose state the fused y pass fetches together (its registers also hold the
+// next stage input).
+#ifndef BASTR_EPI_CHUNK_YFI
+#define BASTR_EPI_CHUNK_YFI 2
+#endif
+#ifndef BASTR_MINB_YFI
+#define BASTR_MINB_YFI 2
+#endif
 #ifndef BASTR_MINB_XPASS
 #define BASTR_MINB_XPASS 0
 #endif
@@ -511,6 +519,150 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
             if (threadIdx.x == 0) io.energy_part[blockIdx.x] = r[0];
         }
     }
+}
+
+
+// ---------------------------------------------------------------------------------------
+// Pass C + A of the next stage: the forward y pass of RK stage 1 or 2 (or a Crank-Nicolson
+// sweep before the last) followed, in the same kernel, by the next stage's inverse y
+// transforms of the stage input it has just formed.  Both transforms use EPT = 8, so the
+// forward transform's output order in registers is the inverse's input order (mirrored
+// plans): the new stage input goes from the epilogue into the inverse without a round trip
+// through HBM, and one pass and one launch per stage disappear.  MA is written in the same
+// [kx][group][y][4] records as pass A (ftot = 4: the stages after the first carry no
+// velocity-gradient fields).
+// ---------------------------------------------------------------------------------------
+template <typename T, int NY> struct YFwdInv2D {
+    static constexpr int EPT = ept_fit<NY, 8>();
+    using FFT = RegFFT<T, NY, EPT, 2, false>;
+    using IFFT = RegFFT<T, NY, EPT, 2, true>;
+    static_assert(FFT::RL == IFFT::R0, "forward output order must be the inverse input order");
+    static constexpr int G = groups_per_block<FFT::NTR>();
+    static constexpr int NT = G * FFT::NTR;
+    static constexpr int MINB = (sizeof(T) == 4 && NT >= 256) ? BASTR_MINB_YFI : 1;
+    static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<T>);
+    static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
+    static constexpr size_t TWB = tw_smem_bytes<T, NY>();
+    static constexpr size_t SMEM = STAGE + XCHR + TWB;
+};
+
+template <typename T, int NY, int EPI>
+__global__ void __launch_bounds__(YFwdInv2D<T, NY>::NT, YFwdInv2D<T, NY>::MINB)
+k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g, const cplx<T>* tw,
+             cplx<T>* __restrict__ MA) {
+    static_assert(EPI == EPI_RK1 || EPI == EPI_RK2 || EPI == EPI_CN_MID, "stages that hand on a stage input");
+    using P = YFwdInv2D<T, NY>;
+    using FFT = typename P::FFT;
+    using IFFT = typename P::IFFT;
+    constexpr int EPT = P::EPT, NT = P::NT, G = P::G;
+    constexpr int W = 4, FTOT = 4;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
+    const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
+    tw = stage_twiddles<T, NY>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
+    pdl_wait();
+    const int K = g.K, KY = g.KY;
+    const int nitems = (K + G - 1) / G;
+    // columns kx0.. of every row (records of two rows in MB) -> staging [col][y][c]
+    auto issue = [&](int item) {
+        const int kx0 = item * G;
+        const int ncol = min(G, K - kx0);
+        constexpr int C16 = 2 * (int)sizeof(cplx<T>) / 16;
+        const int total = NY * G * C16;
+        for (int i = threadIdx.x; i < total; i += NT) {
+            const int q = i / C16, c = i - q * C16;
+            const int col = q % G, y = q / G;
+            if (col < ncol)
+                cp_async16(reinterpret_cast<unsigned char*>(stg) + ((size_t)(col * NY + y) * 2 * sizeof(cplx<T>) + c * 16),
+                           MB + (((size_t)(y >> 1) * K + kx0 + col) * 2 + (y & 1)) * 2 + c * (16 / (int)sizeof(cplx<T>)));
+        }
+        cp_async_commit();
+    };
+    const double inv_n = g.inv_n;
+    const long long K2 = (long long)K * K;
+    double en = 0.0;
+    int item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const cplx<T>* col = stg + (size_t)gi * NY * 2;
+        const int kx = item * G + gi;
+        const bool valid = kx < K;
+        cplx<T> v[2 * EPT];
+#pragma unroll
+        for (int e = 0; e < EPT; ++e) {
+            const int y = FFT::in_pos(t, e);
+            v[e] = valid ? col[2 * y] : mk<T>(0, 0);
+            v[EPT + e] = valid ? col[2 * y + 1] : mk<T>(0, 0);
+        }
+        __syncthreads();   // the staging buffer is free: fetch the next column group now
+        if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        FFT::run(v, sm, tw, t);
+        // the next stage input at the positions this thread holds (zero outside the kept set)
+        cplx<T> nx[2 * EPT];
+#pragma unroll
+        for (int e = 0; e < 2 * EPT; ++e) nx[e] = mk<T>(0, 0);
+        if (valid) {
+            const double w = kx == 0 ? 1.0 : 2.0;
+            const bool from_u0 = input_is_u0 != 0;
+            constexpr int CH = EPT < BASTR_EPI_CHUNK_YFI ? EPT : BASTR_EPI_CHUNK_YFI;
+#pragma unroll
+            for (int e0 = 0; e0 < EPT; e0 += CH) {
+                EpiIn<T, 2> in[CH];
+#pragma unroll
+                for (int j = 0; j < CH; ++j) {
+                    const int kyi = pos_trunc(FFT::out_pos(t, e0 + j), K, KY, NY);
+                    if (kyi >= 0) epi_load<T, 2, EPI>(in[j], ((size_t)kx * KY + kyi) * 2, 1, io, from_u0);
+                }
+#pragma unroll
+                for (int j = 0; j < CH; ++j) {
+                    const int e = e0 + j;
+                    const int kyi = pos_trunc(FFT::out_pos(t, e), K, KY, NY);
+                    if (kyi < 0) continue;
+                    const int ky = trunc_k(kyi, K, KY);
+                    const size_t o = ((size_t)kx * KY + kyi) * 2;
+                    const long long m2i = (long long)kx * kx + (long long)ky * ky;
+                    double2 vv[2];
+                    if (m2i < K2) {   // spherical 2/3 rule, tool.F90:185-193
+                        vv[0] = dscale(cvt<cplx<T>, double2>(v[e]), inv_n);
+                        vv[1] = dscale(cvt<cplx<T>, double2>(v[EPT + e]), inv_n);
+                    } else {
+                        vv[0] = make_double2(0, 0);
+                        vv[1] = make_double2(0, 0);
+                    }
+                    const double kv[2] = {(double)kx, (double)ky};
+                    cplx<T> nxt[2];
+                    rk_apply<T, 2, EPI, true, EPI != EPI_RK1>(vv, kv, (double)m2i, in[j], o, 1, io, from_u0, g, w,
+                                                              en, nxt);
+                    nx[e] = nxt[0];
+                    nx[EPT + e] = nxt[1];
+                }
+            }
+        }
+        // next stage, pass A: g_c = IFFT_y(u_c^), h_c = IFFT_y(i ky u_c^), one sub-pass per component
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            cplx<T> u[2 * EPT];
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+                const int kyi = pos_trunc(IFFT::in_pos(t, e), K, KY, NY);
+                const T ky = (T)(kyi >= 0 ? trunc_k(kyi, K, KY) : 0);
+                u[e] = nx[c * EPT + e];
+                u[EPT + e] = cscale<T>(cmuli<T>(nx[c * EPT + e]), ky);
+            }
+            IFFT::run(u, sm, tw, t);
+            if (valid) {
+                cplx<T>* dst = MA + (size_t)kx * (FTOT / W) * NY * W + 2 * c;
+#pragma unroll
+                for (int e = 0; e < EPT; ++e) st2<T>(dst + (size_t)IFFT::out_pos(t, e) * W, u[e], u[EPT + e]);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    (void)en;
 }
 
 }  // namespace bastr

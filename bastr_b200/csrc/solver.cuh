@@ -163,7 +163,8 @@ __device__ __forceinline__ void epi_load(EpiIn<T, D>& in, size_t o, size_t cst, 
 #pragma unroll
         for (int c = 0; c < D; ++c) {
             in.a[c] = io.u0[o + c * cst];
-            if (!from_u0) in.s[c] = io.us[o + c * cst];
+            // RK2 re-forms its stage input u0 + dt/2 k1 from a and p instead of reading it
+            if (!from_u0 && EPI != EPI_RK2) in.s[c] = io.us[o + c * cst];
             if constexpr (EPI == EPI_RK2 || EPI == EPI_RK3) in.p[c] = io.acc[o + c * cst];
         }
     }
@@ -174,10 +175,13 @@ __device__ __forceinline__ void epi_load(EpiIn<T, D>& in, size_t o, size_t cst, 
 // the advective product; k[c] the wavenumbers, m2 = |k|^2; in the mode's state values
 // (epi_load); o the state offset of component 0; cst the stride between components; w the
 // Hermitian weight of the mode (1 on kx = 0, else 2); en accumulates w*|u0_new|^2.
-template <typename T, int D, int EPI>
+// With NEXT, the new stage input that RK1, RK2 and CN_MID store to io.us is also returned in
+// next[c] (the value stored, in T), for a pass that transforms it on the spot; RK1 then need
+// not store it at all (STORE_US = false), since RK2 re-forms it.
+template <typename T, int D, int EPI, bool NEXT = false, bool STORE_US = true>
 __device__ __forceinline__ void rk_apply(double2* v, const double* k, double m2, const EpiIn<T, D>& in,
                                          size_t o, size_t cst, const StageIO<T>& io, bool from_u0,
-                                         const Geo& g, double w, double& en) {
+                                         const Geo& g, double w, double& en, cplx<T>* next = nullptr) {
     if constexpr (EPI == EPI_STORE) {
 #pragma unroll
         for (int c = 0; c < D; ++c) io.u0[o + c * cst] = v[c];
@@ -186,8 +190,15 @@ __device__ __forceinline__ void rk_apply(double2* v, const double* k, double m2,
         const double nu = g.nu, dt = g.dt;
 #pragma unroll
         for (int c = 0; c < D; ++c) {
-            // + nu * FFT(lap u) with lap u^ = -|k|^2 u^
-            const double2 s = from_u0 ? in.a[c] : cvt<cplx<T>, double2>(in.s[c]);
+            // + nu * FFT(lap u) with lap u^ = -|k|^2 u^ of the stage input (RK2: u0 + dt/2 k1,
+            // the value RK1 formed, exactly so in FP64)
+            double2 s;
+            if constexpr (EPI == EPI_RK2) {
+                const double2 p = cvt<cplx<T>, double2>(in.p[c]);
+                s = make_double2(in.a[c].x + g.dt * p.x / 2.0, in.a[c].y + g.dt * p.y / 2.0);
+            } else {
+                s = from_u0 ? in.a[c] : cvt<cplx<T>, double2>(in.s[c]);
+            }
             v[c].x += nu * (-(s.x * m2));
             v[c].y += nu * (-(s.y * m2));
         }
@@ -217,11 +228,15 @@ __device__ __forceinline__ void rk_apply(double2* v, const double* k, double m2,
             const double2 a = in.a[c];
             if constexpr (EPI == EPI_RK1) {
                 io.acc[o + c * cst] = cvt<double2, cplx<T>>(v[c]);
-                io.us[o + c * cst] = cvt<double2, cplx<T>>(make_double2(a.x + dt * v[c].x / 2.0, a.y + dt * v[c].y / 2.0));
+                const cplx<T> u = cvt<double2, cplx<T>>(make_double2(a.x + dt * v[c].x / 2.0, a.y + dt * v[c].y / 2.0));
+                if constexpr (STORE_US) io.us[o + c * cst] = u;
+                if constexpr (NEXT) next[c] = u;
             } else if constexpr (EPI == EPI_RK2) {
                 const double2 p = cvt<cplx<T>, double2>(in.p[c]);
-                io.us[o + c * cst] = cvt<double2, cplx<T>>(
+                const cplx<T> u = cvt<double2, cplx<T>>(
                     make_double2(a.x - dt * p.x + dt2 * v[c].x, a.y - dt * p.y + dt2 * v[c].y));
+                io.us[o + c * cst] = u;
+                if constexpr (NEXT) next[c] = u;
                 io.acc[o + c * cst] = cvt<double2, cplx<T>>(make_double2(p.x + 4.0 * v[c].x, p.y + 4.0 * v[c].y));
             } else if constexpr (EPI == EPI_RK3) {
                 const double2 p = cvt<cplx<T>, double2>(in.p[c]);
@@ -229,8 +244,10 @@ __device__ __forceinline__ void rk_apply(double2* v, const double* k, double m2,
                 io.u0[o + c * cst] = n;
                 en += w * (n.x * n.x + n.y * n.y);
             } else if constexpr (EPI == EPI_CN_MID) {
-                io.us[o + c * cst] = cvt<double2, cplx<T>>(
+                const cplx<T> u = cvt<double2, cplx<T>>(
                     make_double2(0.5 * ((a.x + dt * v[c].x) + a.x), 0.5 * ((a.y + dt * v[c].y) + a.y)));
+                io.us[o + c * cst] = u;
+                if constexpr (NEXT) next[c] = u;
             } else if constexpr (EPI == EPI_CN_LAST) {
                 const double2 n = make_double2(a.x + dt * v[c].x, a.y + dt * v[c].y);
                 io.u0[o + c * cst] = n;
