@@ -42,6 +42,8 @@ EXPORTED = [
     "bastr_ensemble_create", "bastr_ensemble_destroy", "bastr_ensemble_size", "bastr_ensemble_set_state",
     "bastr_ensemble_get_state", "bastr_ensemble_step", "bastr_ensemble_set_plan", "bastr_ensemble_get_plan",
     "bastr_ensemble_tune", "bastr_ensemble_last_error",
+    "bastr_net_nparams", "bastr_net_grad_blocks", "bastr_net_forward", "bastr_net_grad", "bastr_net_adam",
+    "bastr_closure_apply",
 ]
 BASTR_E_TOO_LARGE = -6
 
@@ -116,6 +118,12 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_ensemble_get_plan.argtypes = [P, C.POINTER(C.c_int32)]
     lib.bastr_ensemble_tune.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, D]
     lib.bastr_ensemble_last_error.argtypes = [P, C.c_char_p, C.c_int32]
+    lib.bastr_net_nparams.argtypes = []
+    lib.bastr_net_grad_blocks.argtypes = []
+    lib.bastr_net_forward.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P, P, C.c_float, P]
+    lib.bastr_net_grad.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P, P, P, C.c_int32, P, P, P]
+    lib.bastr_net_adam.argtypes = [P, P, P, P, P, C.c_int32, C.c_float, C.c_float, C.c_float, C.c_float, P]
+    lib.bastr_closure_apply.argtypes = [P, P, C.c_float, C.c_double]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -264,6 +272,11 @@ class BastrGPU:
 
     def sync(self):
         self._check(self.lib.bastr_sync(self.h))
+
+    def closure_apply(self, net, scale: float, dt: float):
+        """One closure sub-step u <- u - dt * scale * net(u) on this (3D) solver's state; `net` is
+        a bastr_b200.closure.Net."""
+        self._check(self.lib.bastr_closure_apply(self.h, C.c_void_p(net.wb.data_ptr()), C.c_float(scale), dt))
 
     def set_plan(self, share_log2: int):
         """Persistent grids on 1/2**share_log2 of the resident blocks (0 = all)."""

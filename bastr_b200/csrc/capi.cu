@@ -30,6 +30,7 @@
 #include "pass2d.cu"
 #include "pass3d.cu"
 #include "fullfft.cu"
+#include "closure.cu"
 
 using namespace bastr;
 
@@ -71,6 +72,7 @@ struct bastr_handle {
     unsigned int* done = nullptr;  // completion tickets of last-block reductions [kTickets]
     int share_log2 = 0;            // plan: persistent grids use 1/2^share_log2 of the resident blocks
     bool ma_ready = false;         // 2D: MA already holds pass A of the next stage
+    float* closure_buf = nullptr;  // 3D closure: tau_hat [3][n] (allocated on first use)
     double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
     bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
     double* shell = nullptr;   // [nshell][4]
@@ -257,7 +259,7 @@ cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
         cudaError_t e = persistent_grid(h, k, smem, P::NT, cdiv(h->g.K, P::G), &grid);
         if (e != cudaSuccess) return e;
         const double K_ = h->g.K;
-        ProfScope ps(h, SET == YI_VG ? "k2d_yinv_vg" : "k2d_yinv",
+        ProfScope ps(h, SET == YI_VG ? "k2d_yinv_vg" : SET == YI_RHS_VG ? "k2d_yinv_rhs_vg" : "k2d_yinv",
                      K_ * h->g.KY * 2 * sizeof(cplx<TIN>) + (double)h->g.ny * K_ * P::F * sizeof(cplx<T>));
         LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[1])));
     });
@@ -330,13 +332,16 @@ template <typename T>
 cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
     cudaError_t e = cudaSuccess;
     const int ftot = vg ? 8 : 4;
-    if (from_u0) e = l2_yinv<T, double, YI_RHS>(h, h->u0, h->ma, ftot);
+    if (from_u0 && vg) e = l2_yinv<T, double, YI_RHS_VG>(h, h->u0, h->ma, ftot);
+    else if (from_u0) e = l2_yinv<T, double, YI_RHS>(h, h->u0, h->ma, ftot);
     else if (!h->ma_ready || vg) e = l2_yinv<T, T, YI_RHS>(h, h->us, h->ma, ftot);
     h->ma_ready = false;
     if (e != cudaSuccess) return e;
     if (vg) {
-        e = l2_yinv<T, double, YI_VG>(h, h->u0, h->ma, ftot);
-        if (e != cudaSuccess) return e;
+        if (!from_u0) {   // the statistics are of the state u0
+            e = l2_yinv<T, double, YI_VG>(h, h->u0, h->ma, ftot);
+            if (e != cudaSuccess) return e;
+        }
         e = l2_xpass<T, XM_RHS_VG>(h, h->ma, ftot, h->mb, nullptr, nullptr, h->vg_part);
     } else {
         e = l2_xpass<T, XM_RHS>(h, h->ma, ftot, h->mb, nullptr, nullptr, nullptr);
@@ -650,6 +655,7 @@ int count_launches(bastr_handle* h, bool vg) {
     const int nrhs = h->p.timemethod == 1 ? 3 : 6;
     n += per_rhs * nrhs;
     if (h->g.d == 2 && BASTR_FUSE_Y) n -= nrhs - 1;  // pass A of every stage but the first is fused
+    if (h->g.d == 2 && vg) n -= 1;                   // 2D: one pass A makes the product and statistics fields
     if (vg) n += 2;                                 // extra inverse pass + final reduction
     const int m = h->p.forcemethod;
     if (m == 1) n += 1;
@@ -715,7 +721,7 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
 }
 
 void free_all(bastr_handle* h) {
-    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend,
+    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->closure_buf,
                     h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
                     h->sp_item_part};
     for (void* q : ptrs)
@@ -1174,6 +1180,70 @@ int bastr_last_error(bastr_handle* h, char* buf, int32_t n) {
         buf[m] = 0;
     }
     return len;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int bastr_net_nparams(void) { return kNetNP; }
+
+int bastr_net_grad_blocks(void) { return 2 * 148; }
+
+int bastr_net_forward(int32_t nx, int32_t ny, int32_t nz, const float* d_u, const uint16_t* d_w, float* d_out,
+                      float scale, void* stream) {
+    if (nx < 3 || ny < 3 || nz < 3 || !d_u || !d_w || !d_out) return BASTR_E_INVALID;
+    const size_t n = (size_t)nx * ny * nz;
+    const int grid = (int)std::min<size_t>((n + 127) / 128, 148 * 8);
+    k_net_forward<float><<<grid, 128, 0, (cudaStream_t)stream>>>(d_u, (const __nv_bfloat16*)d_w, d_out, nx, ny, nz,
+                                                                  scale);
+    return cudaGetLastError() == cudaSuccess ? BASTR_OK : BASTR_E_CUDA;
+}
+
+int bastr_net_grad(int32_t nx, int32_t ny, int32_t nz, const float* d_u, const float* d_tau, const uint16_t* d_w,
+                   float* d_part, int32_t nblk, float* d_grad, double* d_loss, void* stream) {
+    if (nx < 3 || ny < 3 || nz < 3 || !d_u || !d_tau || !d_w || !d_part || !d_grad || nblk < 1)
+        return BASTR_E_INVALID;
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_net_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGradSmem);
+    });
+    if (attr != cudaSuccess) return BASTR_E_CUDA;
+    const size_t n = (size_t)nx * ny * nz;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_net_grad<<<nblk, kGradNT, kGradSmem, st>>>(d_u, d_tau, (const __nv_bfloat16*)d_w, d_part, nx, ny, nz);
+    k_net_reduce<<<(kNetNP + 1 + 255) / 256, 256, 0, st>>>(d_part, nblk, d_grad, d_loss, 1.0 / (3.0 * (double)n));
+    return cudaGetLastError() == cudaSuccess ? BASTR_OK : BASTR_E_CUDA;
+}
+
+int bastr_net_adam(float* d_w, uint16_t* d_wb, float* d_m, float* d_v, const float* d_g, int32_t t, float lr,
+                   float b1, float b2, float eps, void* stream) {
+    if (!d_w || !d_wb || !d_m || !d_v || !d_g || t < 1) return BASTR_E_INVALID;
+    k_net_adam<<<(kNetNP + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_w, (__nv_bfloat16*)d_wb, d_m, d_v, d_g, t,
+                                                                       lr, b1, b2, eps);
+    return cudaGetLastError() == cudaSuccess ? BASTR_OK : BASTR_E_CUDA;
+}
+
+// One closure sub-step on a 3D handle's state: u <- u - dt * scale * net(u) in physical space,
+// then back to the (dealiased) spectral state.
+int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float scale, double dt) {
+    if (!h || !d_w) return BASTR_E_INVALID;
+    if (h->g.d != 3) return fail(h, BASTR_E_UNSUPPORTED, "the closure network is three-dimensional");
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    CK(cudaSetDevice(h->device));
+    const size_t n = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    if (!h->closure_buf) CK(cudaMalloc(&h->closure_buf, 3 * n * sizeof(float)));
+    CK(flush_pending_scale(h));
+    CK(to_physical(h));
+    const int grid = (int)std::min<size_t>((n + 127) / 128, 148 * 8);
+    k_net_forward<double><<<grid, 128, 0, h->stream>>>(h->phys, (const __nv_bfloat16*)d_w, h->closure_buf, h->g.nx,
+                                                        h->g.ny, h->g.nz, scale);
+    CK(cudaGetLastError());
+    k_closure_update<<<148 * 4, 256, 0, h->stream>>>(h->phys, h->closure_buf, 3 * n, dt);
+    CK(cudaGetLastError());
+    CK(to_spectral(h));
+    return BASTR_OK;
 }
 
 }  // extern "C"

@@ -89,11 +89,13 @@ template <typename T> __device__ __forceinline__ void st2(cplx<T>* dst, cplx<T> 
 // ---------------------------------------------------------------------------------------
 // Pass A: inverse transforms along y of kx columns.
 // ---------------------------------------------------------------------------------------
-enum YInvSet : int { YI_STATE = 0, YI_RHS = 1, YI_VG = 2 };
+// Field sets: the state (u1, u2), the product's fields (g1, h1, g2, h2), the velocity-gradient
+// fields (q1, q2, t), or both of the last two from one read of the column (YI_RHS_VG).
+enum YInvSet : int { YI_STATE = 0, YI_RHS = 1, YI_VG = 2, YI_RHS_VG = 3 };
 
 template <typename T, typename TIN, int NY, int SET> struct YInv2D {
-    static constexpr int F = SET == YI_STATE ? 2 : SET == YI_RHS ? 4 : 3;   // fields produced
-    static constexpr int F0 = SET == YI_VG ? 4 : 0;                          // offset in MA
+    static constexpr int F = SET == YI_STATE ? 2 : SET == YI_RHS ? 4 : SET == YI_VG ? 3 : 7;   // fields produced
+    static constexpr int F0 = SET == YI_VG ? 4 : 0;                                             // offset in MA
     static constexpr int UG = 2;                                             // units per sub-pass
     static constexpr int NG = (F + UG - 1) / UG;
     static constexpr int EPT = ept_fit<NY, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_YINV_F32>();
@@ -160,20 +162,22 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
                 const int kyi = pos_trunc(FFT::in_pos(t, e), K, KY, NY);
                 const T ky = (T)(kyi >= 0 ? trunc_k(kyi, K, KY) : 0);
                 const cplx<T> a = ra[e], b = rb[e];
-                cplx<T> f[4];
+                cplx<T> f[8];
                 if constexpr (SET == YI_STATE) {
                     f[0] = a; f[1] = b; f[2] = f[3] = mk<T>(0, 0);
-                } else if constexpr (SET == YI_RHS) {
+                } else if constexpr (SET == YI_RHS || SET == YI_RHS_VG) {
                     f[0] = a; f[1] = cscale<T>(cmuli<T>(a), ky);
                     f[2] = b; f[3] = cscale<T>(cmuli<T>(b), ky);
-                } else {
+                }
+                if constexpr (SET == YI_VG || SET == YI_RHS_VG) {
+                    constexpr int o = SET == YI_VG ? 0 : 4;
                     const T ky2 = ky * ky;
-                    f[0] = cscale<T>(a, ky2);
-                    f[1] = cscale<T>(b, ky2);
+                    f[o + 0] = cscale<T>(a, ky2);
+                    f[o + 1] = cscale<T>(b, ky2);
                     // lap(theta)^ = -i |k|^2 (kx u1^ + ky u2^)   (solution.F90:1131)
                     const T kk = kxt * kxt + ky2;
-                    f[2] = cscale<T>(cmulni<T>(cadd<T>(cscale<T>(a, kxt), cscale<T>(b, ky))), kk);
-                    f[3] = mk<T>(0, 0);
+                    f[o + 2] = cscale<T>(cmulni<T>(cadd<T>(cscale<T>(a, kxt), cscale<T>(b, ky))), kk);
+                    f[o + 3] = mk<T>(0, 0);
                 }
 #pragma unroll
                 for (int u = 0; u < UG; ++u) v[u * EPT + e] = f[grp * UG + u];

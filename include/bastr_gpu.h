@@ -189,6 +189,31 @@ BASTR_API int bastr_ensemble_tune(bastr_ensemble* e, int32_t nsteps, int32_t rep
                                   double* best_ms);
 BASTR_API int bastr_ensemble_last_error(bastr_ensemble* e, char* buf, int32_t n);
 
+/* ------------------------------------------------------------------------------------------
+ * Learned subgrid closure for a coarse 3D solve (no reference counterpart).  A local network
+ * (3x3x3 stencil 3->32, then 1x1x1 32->32, 32->32, 32->3; GELU; BF16 weights, FP32 sums)
+ * maps the velocity u [3][nz][ny][nx] to the subgrid term tau.  Device pointers; weights are
+ * bastr_net_nparams() BF16 values (uint16_t bit patterns) with FP32 master copies for training.
+ *
+ *   bastr_net_forward   out = scale * net(u)
+ *   bastr_net_grad      loss = mean((net(u) - tau)^2) and its gradient; d_part: workspace of
+ *                       nblk * (nparams + 1) floats (nblk: e.g. bastr_net_grad_blocks()); the
+ *                       result is deterministic for a given nblk
+ *   bastr_net_adam      one Adam step on the FP32 weights; refreshes the BF16 copy
+ *   bastr_closure_apply one sub-step u <- u - dt * scale * net(u) on a 3D handle's state
+ *                       (physical space, then back to the dealiased spectral state)
+ * ------------------------------------------------------------------------------------------ */
+BASTR_API int bastr_net_nparams(void);
+BASTR_API int bastr_net_grad_blocks(void);
+BASTR_API int bastr_net_forward(int32_t nx, int32_t ny, int32_t nz, const float* d_u, const uint16_t* d_w,
+                                float* d_out, float scale, void* stream);
+BASTR_API int bastr_net_grad(int32_t nx, int32_t ny, int32_t nz, const float* d_u, const float* d_tau,
+                             const uint16_t* d_w, float* d_part, int32_t nblk, float* d_grad, double* d_loss,
+                             void* stream);
+BASTR_API int bastr_net_adam(float* d_w, uint16_t* d_wb, float* d_m, float* d_v, const float* d_g, int32_t t,
+                             float lr, float b1, float b2, float eps, void* stream);
+BASTR_API int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float scale, double dt);
+
 #ifdef __cplusplus
 }
 #endif
