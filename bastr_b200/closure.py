@@ -108,17 +108,33 @@ class Net:
         if rc != 0:
             raise RuntimeError(f"bastr_net_adam: {rc}")
 
-    def train(self, pairs, iters: int, lr: float = 2e-3, log_every: int = 0):
-        """Adam over the (u, tau/tau_scale) pairs in turn; returns the loss history."""
+    def train(self, pairs, iters: int, lr: float = 2e-3, log_every: int = 0, group=None):
+        """Adam over the (u, tau/tau_scale) pairs in turn; returns the loss history.  With a
+        torch.distributed process group of several ranks (one GPU each, every rank holding its
+        own pairs), the gradient is averaged over the ranks before every step (data parallel:
+        one all-reduce of the nparams() floats per step)."""
         hist = []
         for it in range(iters):
             u, tau = pairs[it % len(pairs)]
-            loss, _ = self.loss_grad(u, tau)
+            loss, g = self.loss_grad(u, tau)
+            if group is not None:
+                average_gradient(g, group)
             self.adam(lr)
             hist.append(loss)
             if log_every and it % log_every == 0:
                 print(f"iter {it}: loss {loss:.4e}", flush=True)
         return hist
+
+
+def average_gradient(g, group=None):
+    """In-place mean of a gradient tensor over the ranks of a torch.distributed group (NCCL for
+    CUDA tensors, gloo for CPU tensors)."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    if world > 1:
+        dist.all_reduce(g, op=dist.ReduceOp.SUM, group=group)
+        g.div_(world)
+    return g
 
 
 # ---------------------------------------------------------------------------------------------
