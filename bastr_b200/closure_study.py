@@ -86,10 +86,11 @@ def run(args) -> dict:
             c.set_state(ub0)
 
             def go():   # no host round trip per step: records are not read back
-                for _ in range(args.steps):
+                for i in range(args.steps):
                     c.step_async(1)
-                    if closure:
-                        c.closure_apply(net, tau_rms, args.dt)
+                    if closure and (i + 1) % args.closure_every == 0:
+                        # one split sub-step covering the last closure_every steps
+                        c.closure_apply(net, tau_rms, args.dt * args.closure_every)
                 c.sync()
             _, t = _sync_time(go)
             return coarse_spectrum(c.get_state()), t
@@ -109,6 +110,7 @@ def run(args) -> dict:
         "fine": nf, "coarse": nc, "filter_width_cells": r, "reynolds": args.reynolds, "dt": args.dt,
         "train_seeds": args.train_seeds, "test_seed": args.test_seed, "pairs": len(pairs),
         "spinup_steps": args.spinup, "test_steps": args.steps, "iters": args.iters, "tau_rms": tau_rms,
+        "closure_every": args.closure_every,
         "loss_first": hist[0], "loss_last": hist[-1], "train_gpu_s": t_train,
         "fine_gpu_s": t_fine, "coarse_plain_gpu_s": t_plain, "coarse_closure_gpu_s": t_clos,
         "speedup_closure_vs_fine": t_fine / t_clos,
@@ -135,6 +137,8 @@ def main():
     ap.add_argument("--iters", type=int, default=2000)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--net-seed", type=int, default=0)
+    ap.add_argument("--closure-every", type=int, default=1,
+                    help="apply the closure once every this many coarse steps (sub-step dt times it)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     res = run(args)
