@@ -43,7 +43,7 @@ EXPORTED = [
     "bastr_ensemble_get_state", "bastr_ensemble_step", "bastr_ensemble_set_plan", "bastr_ensemble_get_plan",
     "bastr_ensemble_tune", "bastr_ensemble_last_error",
     "bastr_net_nparams", "bastr_net_grad_blocks", "bastr_net_forward", "bastr_net_grad", "bastr_net_adam",
-    "bastr_closure_apply",
+    "bastr_closure_apply", "bastr_transfer",
 ]
 BASTR_E_TOO_LARGE = -6
 
@@ -124,6 +124,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_net_grad.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P, P, P, C.c_int32, P, P, P]
     lib.bastr_net_adam.argtypes = [P, P, P, P, P, C.c_int32, C.c_float, C.c_float, C.c_float, C.c_float, P]
     lib.bastr_closure_apply.argtypes = [P, P, C.c_float, C.c_double]
+    lib.bastr_transfer.argtypes = [P, D, D, D]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -272,6 +273,14 @@ class BastrGPU:
 
     def sync(self):
         self._check(self.lib.bastr_sync(self.h))
+
+    def transfer(self):
+        """Transfer spectra T, T1, T2 of the current state, shells 0..allkmax (Bastrpp's
+        transfer2d/transfer3d)."""
+        n = self.allkmax + 1
+        t, t1, t2 = (np.empty(n) for _ in range(3))
+        self._check(self.lib.bastr_transfer(self.h, _dptr(t), _dptr(t1), _dptr(t2)))
+        return t, t1, t2
 
     def closure_apply(self, net, scale: float, dt: float):
         """One closure sub-step u <- u - dt * scale * net(u) on this (3D) solver's state; `net` is

@@ -31,6 +31,7 @@
 #include "pass3d.cu"
 #include "fullfft.cu"
 #include "closure.cu"
+#include "transfer.cu"
 
 using namespace bastr;
 
@@ -73,6 +74,8 @@ struct bastr_handle {
     int share_log2 = 0;            // plan: persistent grids use 1/2^share_log2 of the resident blocks
     bool ma_ready = false;         // 2D: MA already holds pass A of the next stage
     float* closure_buf = nullptr;  // 3D closure: tau_hat [3][n] (allocated on first use)
+    double2* tr_buf = nullptr;     // transfer spectra: full complex grids (allocated on first use)
+    double* tr_modes = nullptr;    // transfer spectra: per-mode values, item partials, shell sums
     double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
     bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
     double* shell = nullptr;   // [nshell][4]
@@ -721,7 +724,7 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
 }
 
 void free_all(bastr_handle* h) {
-    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->closure_buf,
+    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->closure_buf, h->tr_buf, h->tr_modes,
                     h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
                     h->sp_item_part};
     for (void* q : ptrs)
@@ -1223,6 +1226,65 @@ int bastr_net_adam(float* d_w, uint16_t* d_wb, float* d_m, float* d_v, const flo
     k_net_adam<<<(kNetNP + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_w, (__nv_bfloat16*)d_wb, d_m, d_v, d_g, t,
                                                                        lr, b1, b2, eps);
     return cudaGetLastError() == cudaSuccess ? BASTR_OK : BASTR_E_CUDA;
+}
+
+// Transfer spectra of the current state (transfer2d/transfer3d, Bastrpp.F90:174-305, 418-599):
+// T, T1, T2 for shells 0..allkmax (host arrays of allkmax+1 doubles).
+int bastr_transfer(bastr_handle* h, double* T, double* T1, double* T2) {
+    if (!h) return BASTR_E_INVALID;
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    CK(cudaSetDevice(h->device));
+    const Geo& g = h->g;
+    const int D = g.d;
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    const size_t narr = (size_t)(D + D * D + D + D + D * D);
+    const size_t nmodes = (size_t)g.K * g.KY * g.KZ;
+    if (!h->tr_buf) CK(cudaMalloc(&h->tr_buf, narr * n * sizeof(double2)));
+    if (!h->tr_modes)
+        CK(cudaMalloc(&h->tr_modes, (nmodes * 3 + (size_t)std::max(h->n_items, 1) * 3 + 3 * (size_t)h->nshell) *
+                                        sizeof(double)));
+    double2* U = h->tr_buf;
+    double2* Dv = U + (size_t)D * n;
+    double2* tA = Dv + (size_t)D * D * n;
+    double2* tC = tA + (size_t)D * n;
+    double2* P = tC + (size_t)D * n;
+    double* tr = h->tr_modes;
+    double* part = tr + nmodes * 3;
+    double* out = part + (size_t)std::max(h->n_items, 1) * 3;
+    CK(flush_pending_scale(h));
+    CK(cudaMemsetAsync(U, 0, (size_t)D * n * sizeof(double2), h->stream));
+    const int gs = 148 * 8;
+    if (D == 2) k_tr_scatter<2><<<gs, 256, 0, h->stream>>>(h->u0, g, U, n);
+    else k_tr_scatter<3><<<gs, 256, 0, h->stream>>>(h->u0, g, U, n);
+    CK(cudaGetLastError());
+    for (int c = 0; c < D; ++c)
+        for (int j = 0; j < D; ++j) k_tr_deriv<<<gs, 256, 0, h->stream>>>(U + (size_t)c * n, Dv + (size_t)(c * D + j) * n, j, g);
+    CK(cudaGetLastError());
+    // to physical space: u_c and d_cj
+    for (size_t a = 0; a < (size_t)(D + D * D); ++a)
+        for (int ax = 0; ax < D; ++ax) CK(full_axis<true>(h, U + a * n, ax, 1.0));
+    if (D == 2) k_tr_products<2><<<gs, 256, 0, h->stream>>>(U, Dv, tA, tC, P, n);
+    else k_tr_products<3><<<gs, 256, 0, h->stream>>>(U, Dv, tA, tC, P, n);
+    CK(cudaGetLastError());
+    // forward transforms (scaled 1/N) of tA, tC, P
+    for (size_t a = 0; a < (size_t)(D + D + D * D); ++a)
+        for (int ax = 0; ax < D; ++ax) CK(full_axis<false>(h, tA + a * n, ax, ax == D - 1 ? g.inv_n : 1.0));
+    if (D == 2) k_tr_modes<2><<<gs, 256, 0, h->stream>>>(h->u0, g, tA, tC, P, tr, n);
+    else k_tr_modes<3><<<gs, 256, 0, h->stream>>>(h->u0, g, tA, tC, P, tr, n);
+    CK(cudaGetLastError());
+    if (h->n_items > 0) k_tr_items<256><<<h->n_items, 256, 0, h->stream>>>(tr, h->sp_modes, h->sp_item_lo, part);
+    else CK(cudaMemsetAsync(part, 0, 3 * sizeof(double), h->stream));
+    k_tr_shells<<<(h->nshell + 127) / 128, 128, 0, h->stream>>>(part, h->sp_shell_item, h->nshell, out);
+    CK(cudaGetLastError());
+    std::vector<double> buf(3 * (size_t)h->nshell);
+    CK(cudaMemcpyAsync(buf.data(), out, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double* dst[3] = {T, T1, T2};
+    for (int k = 0; k < 3; ++k) {
+        if (!dst[k]) continue;
+        for (int s2 = 0; s2 <= h->allkmax; ++s2) dst[k][s2] = s2 < h->nshell ? buf[(size_t)k * h->nshell + s2] : 0.0;
+    }
+    return BASTR_OK;
 }
 
 // One closure sub-step on a 3D handle's state: u <- u - dt * scale * net(u) in physical space,

@@ -308,6 +308,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 const int k = lo ? p : NX - p;
 #pragma unroll
                 for (int u = 0; u < ZU; ++u) v[u * EPT + e] = mk<T>(0, 0);
+                // K = floor(NX/3) in 2D: these elements are dealiased zeros for every thread
+                if (IFFT::in_band(e, NX / 3 + 1)) continue;
                 if (valid && (lo || hi)) {
                     const cplx<T>* src0 = row + (size_t)k * (FIN / W) * G * W;
                     auto src = [&](int f) { return src0[(f / W) * G * W + (f % W)]; };
@@ -386,7 +388,11 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
             FFFT::run(v, sm, tw, t);
             // split the packed spectrum into the two half spectra, kx in [0,K): Z[k] and Z[NX-k]
 #pragma unroll
-            for (int e = 0; e < EPT; ++e) sm[pidx(FFFT::out_pos(t, e))] = v[e];
+            for (int e = 0; e < EPT; ++e) {
+                // outputs strictly between K-1 and NX-K+1 are never read by the split below
+                if (MODE != XM_FROM_PHYS && FFFT::out_band(e, NX / 3 + 1)) continue;
+                sm[pidx(FFFT::out_pos(t, e))] = v[e];
+            }
             __syncthreads();
             if (valid) {
                 for (int k = t; k < K; k += NTR) {

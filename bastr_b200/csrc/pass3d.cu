@@ -346,6 +346,8 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
                 const int k = lo ? p : NX - p;
 #pragma unroll
                 for (int u = 0; u < ZU; ++u) v[u * EPT + e] = mk<T>(0, 0);
+                // K = floor(NX/3): these elements are dealiased zeros for every thread
+                if (IFFT::in_band(e, NX / 3 + 1)) continue;
                 if (valid && (lo || hi)) {
                     const cplx<T>* src0 = rw + (size_t)k * FIN * G;
                     auto src = [&](int f) { return src0[f * G]; };
@@ -435,6 +437,7 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
             constexpr int US = IFFT::US;
 #pragma unroll
             for (int e = 0; e < EPT; ++e) {
+                if (FFFT::out_band(e, NX / 3 + 1)) continue;   // never read by the split below
                 const int x = FFFT::out_pos(t, e);
                 sm[pidx(x)] = v[e];
                 sm[US + pidx(x)] = v[EPT + e];

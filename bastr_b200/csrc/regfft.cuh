@@ -56,6 +56,19 @@ struct RegFFT {
         return t + (e / RL) * NTR + (e % RL) * (N / RL);
     }
 
+    // True when register element e lies, for every thread, in the open band (lo, N - lo) of
+    // positions before the first stage (in_pos) / after the last stage (out_pos): known at
+    // compile time once the loops are unrolled, so a caller can leave such inputs at zero and
+    // skip such outputs, and the compiler folds the arithmetic they would take.
+    __host__ __device__ static constexpr bool in_band(int e, int lo) {
+        const int b = (e / R0) * NTR + (e % R0) * (N / R0);
+        return b >= lo && b + NTR - 1 <= N - lo;
+    }
+    __host__ __device__ static constexpr bool out_band(int e, int lo) {
+        const int b = (e / RL) * NTR + (e % RL) * (N / RL);
+        return b >= lo && b + NTR - 1 <= N - lo;
+    }
+
     template <int R, int PS>
     __device__ static __forceinline__ void compute(cplx<T>* v, const cplx<T>* __restrict__ tw, int t) {
 #pragma unroll

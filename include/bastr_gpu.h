@@ -108,6 +108,12 @@ BASTR_API int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out
 /* Shell spectra of the current state: arrays of allkmax+1 entries (shell 0..allkmax). */
 BASTR_API int bastr_spectra(bastr_handle* h, double* kn, double* Es, double* Ed, int64_t* Ecount);
 
+/* Energy transfer spectra of the current state, Bastrpp's transfer2d/transfer3d
+ * (Bastrpp.F90:174-305, 418-599): T (advective form), T1 (conservative form) and T2 (the
+ * u_i div(u) part) per shell nint(|k|) = 0..allkmax (host arrays of allkmax+1; any may be NULL).
+ * Allocates its full-grid work buffers on the first call (about (2d + 2d^2) complex grids). */
+BASTR_API int bastr_transfer(bastr_handle* h, double* T, double* T1, double* T2);
+
 /* In-place c2c transform of a full complex(8) grid (interleaved re,im; x fastest):
  * dir = -1 forward scaled by 1/N (fft2d/fft3d), dir = +1 backward unscaled (ifft2d/ifft3d). */
 BASTR_API int bastr_fft(bastr_handle* h, double* array, int32_t dir);

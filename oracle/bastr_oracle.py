@@ -451,3 +451,39 @@ def fortran_e20_13(x: float) -> str:
 def listwrite_line(nstep: int, time: float, *vals: float) -> str:
     """utility.F90:87-164: ``(1X,I20,n(1X,E20.13E2))`` with time/ref_tim (ref_tim = 1)."""
     return " " + f"{nstep:20d}" + "".join(" " + fortran_e20_13(v) for v in (time, *vals))
+
+
+# ---------------------------------------------------------------------------------------
+# post-processing: energy transfer spectra (Bastrpp)
+# ---------------------------------------------------------------------------------------
+def transfer(p: Params, u):
+    """transfer2d / transfer3d, Bastrpp.F90:174-305 / 418-599, on the physical field u (list of
+    d real arrays): complex-to-complex transforms with the reference's scaling (forward 1/N,
+    backward unscaled), products in physical space kept complex as the reference keeps them,
+    per-mode trans, trans1, trans2 summed over the full grid into shells kint(|k|) <= allkmax.
+    Returns T, T1, T2 for shells 0..allkmax."""
+    d = p.ndims
+    n = p.npts
+    ks = generate_wave(p)
+    fwd = lambda a: np.fft.fftn(a) / n        # noqa: E731  fft2d/fft3d (fftwlink.F90:324-347)
+    bwd = lambda a: np.fft.ifftn(a) * n       # noqa: E731  ifft2d/ifft3d (fftwlink.F90:349-368)
+    uspe = [fwd(np.asarray(c, dtype=np.complex128)) for c in u]
+    ux = [[bwd(1j * uspe[c] * ks[j]) for j in range(d)] for c in range(d)]
+    uph = [bwd(uspe[c]) for c in range(d)]
+    tA = [-sum(uph[j] * ux[c][j].real for j in range(d)) for c in range(d)]
+    div = sum(ux[j][j] for j in range(d)).real
+    tC = [uph[c] * div for c in range(d)]
+    P = [[uph[c] * uph[j] for j in range(d)] for c in range(d)]
+    tA = [fwd(a) for a in tA]
+    us2 = [fwd(a) for a in uph]
+    tC = [fwd(a) for a in tC]
+    P = [[fwd(a) for a in row] for row in P]
+    trans = sum(np.real(np.conj(us2[c]) * tA[c]) for c in range(d))
+    trans1 = np.imag(sum(ks[j] * P[c][j] * np.conj(us2[c]) for c in range(d) for j in range(d)))
+    trans2 = sum(np.real(np.conj(us2[c]) * tC[c]) for c in range(d))
+    kk = np.sqrt(sum(k * k for k in ks))
+    sh = kint(kk).ravel()
+    am = p.allkmax
+    sel = sh <= am
+    out = [np.bincount(sh[sel], weights=t.ravel()[sel], minlength=am + 1) for t in (trans, trans1, trans2)]
+    return tuple(out)

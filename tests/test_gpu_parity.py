@@ -128,3 +128,24 @@ def test_linear_forcing_state_between_steps(gpu_lib, dims):
             assert rel_l2([r.Esspe for r in recs], [r.Esspe for r in ref]) <= 1e-12
             assert rel_l2([r.factor for r in recs], [r.forcing[0] for r in ref]) <= 1e-12
             assert rel_l2(np.stack(s.get_state()), np.stack(o.u)) <= 1e-12
+
+
+@pytest.mark.parametrize("dims", [(64, 64, 0), (32, 32, 32)], ids=["2d", "3d"])
+def test_transfer_spectra_match_oracle(gpu_lib, dims):
+    """bastr_transfer (Bastrpp transfer2d/transfer3d) against the oracle's restatement on the
+    state after a few steps: every shell 1..allkmax of T, T1, T2 within 1e-12 relative L2."""
+    import numpy as np
+    from bastr_b200 import BastrGPU
+    from oracle.bastr_oracle import transfer
+    from tests.parity_util import rel_l2
+    ia, ja, ka = dims
+    p = make_params(ia, ja, ka, reynolds=2000.0, deltat=1e-3, forcemethod=1, target_energy=1.0)
+    u = field(ia, ja, ka, k0=3.0, seed=5)
+    with BastrGPU(ia, ja, ka, reynolds=p.reynolds, deltat=p.deltat, forcemethod=1, target_energy=1.0) as s:
+        s.set_state(u)
+        s.step(3)
+        uf = s.get_state()
+        got = s.transfer()
+    ref = transfer(p, uf)
+    for g, r in zip(got, ref):
+        assert rel_l2(g[1:], r[1:]) <= 1e-12, (g[1:6], r[1:6])
