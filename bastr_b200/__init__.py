@@ -69,6 +69,7 @@ class CStepOut(C.Structure):
         ("nstep", C.c_int64), ("time", C.c_double),
         ("Esspe", C.c_double), ("Edspe", C.c_double), ("k2Edspe", C.c_double), ("kMEdspe", C.c_double),
         ("velgrad", C.c_double * 8), ("factor", C.c_double), ("E", C.c_double),
+        ("energy", C.c_double), ("Fen", C.c_double),
     ]
 
 
@@ -146,6 +147,8 @@ class StepRecord:
     velgrad: tuple
     factor: float
     E: float
+    energy: float = float("nan")
+    Fen: float = float("nan")
 
 
 def miucal(temper: float, ref_tem: float) -> float:
@@ -251,7 +254,7 @@ class BastrGPU:
     @staticmethod
     def _rec(o: CStepOut) -> StepRecord:
         return StepRecord(o.nstep, o.time, o.Esspe, o.Edspe, o.k2Edspe, o.kMEdspe,
-                          tuple(o.velgrad), o.factor, o.E)
+                          tuple(o.velgrad), o.factor, o.E, o.energy, o.Fen)
 
     def step(self, nsteps: int = 1, shells: bool = False):
         """Runs nsteps main-loop iterations; returns records (and per-step Es/Ed shells)."""

@@ -77,6 +77,7 @@ struct bastr_handle {
     double2* tr_buf = nullptr;     // transfer spectra: full complex grids (allocated on first use)
     double* tr_modes = nullptr;    // transfer spectra: per-mode values, item partials, shell sums
     double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
+    unsigned long long* rng = nullptr;  // forcing calls so far: counter of the random-phase stream
     bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
     double* shell = nullptr;   // [nshell][4]
     double* rec = nullptr;     // [kChunk][R_COUNT]
@@ -352,7 +353,7 @@ cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
     if (e != cudaSuccess) return e;
     StageIO<T> io{h->u0, (cplx<T>*)h->us, (cplx<T>*)h->acc, nullptr};
     const bool need_en = (epi == EPI_RK3 || epi == EPI_CN_LAST) &&
-                         (h->p.forcemethod == 1 || h->p.forcemethod == 5);
+                         (h->p.forcemethod == 1 || h->p.forcemethod >= 3);
     if (need_en) io.energy_part = h->en_part;
     if (BASTR_FUSE_Y && (epi == EPI_RK1 || epi == EPI_RK2 || epi == EPI_CN_MID)) {
         h->ma_ready = true;
@@ -503,7 +504,7 @@ cudaError_t rhs3d(bastr_handle* h, int epi, bool from_u0, bool vg) {
     if (e != cudaSuccess) return e;
     StageIO<T> io{h->u0, (cplx<T>*)h->us, (cplx<T>*)h->acc, nullptr};
     const bool need_en = (epi == EPI_RK3 || epi == EPI_CN_LAST) &&
-                         (h->p.forcemethod == 1 || h->p.forcemethod == 5);
+                         (h->p.forcemethod == 1 || h->p.forcemethod >= 3);
     if (need_en) io.energy_part = h->en_part;
     switch (epi) {
         case EPI_RK1: return l3_zfwd<T, EPI_RK1>(h, h->ma, io, from_u0);
@@ -607,7 +608,7 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec) {
         h->scale_pending = true;
         return cudaGetLastError();
     }
-    if (m == 5) {
+    if (m >= 3) {
         ProfScope ps(h, "k_sum_partials", (double)h->n_en_blocks * 8);
         LAUNCH(launch_k(h, k_sum_partials<256>, 1, 256, 0, h->en_part, h->n_en_blocks, 1.0, rec, R_ENERGY));
     }
@@ -615,9 +616,11 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec) {
         const int proj = (m == 5 && h->g.d == 2 && h->p.lprojectd) ? 1 : 0;
         ProfScope ps(h, "k_force_band", 0);
         if (h->g.d == 2)
-            LAUNCH(launch_k(h, k_force_band<2, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec));
+            LAUNCH(launch_k(h, k_force_band<2, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
+                            h->rng));
         else
-            LAUNCH(launch_k(h, k_force_band<3, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec));
+            LAUNCH(launch_k(h, k_force_band<3, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
+                            h->rng));
     }
     return cudaGetLastError();
 }
@@ -663,6 +666,7 @@ int count_launches(bastr_handle* h, bool vg) {
     const int m = h->p.forcemethod;
     if (m == 1) n += 1;
     else if (m == 2) n += 1;
+    else if (m == 3 || m == 4) n += 2;
     else if (m == 5) n += 2;
     return n;
 }
@@ -724,7 +728,7 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
 }
 
 void free_all(bastr_handle* h) {
-    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->closure_buf, h->tr_buf, h->tr_modes,
+    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->rng, h->closure_buf, h->tr_buf, h->tr_modes,
                     h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
                     h->sp_item_part};
     for (void* q : ptrs)
@@ -787,10 +791,6 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     *out = h;   // also on failure, so that the caller can read the message; destroy it either way
     if (p->ja == 0) return fail(h, BASTR_E_INVALID, "1D case is not implemented yet!");
     if (p->timemethod != 1 && p->timemethod != 2) { int r = fail(h, BASTR_E_INVALID, "Undefined time method"); return r; }
-    if (p->forcemethod == 3 || p->forcemethod == 4) {
-        int r = fail(h, BASTR_E_UNSUPPORTED, "forcemethod %d (random-phase forcing) is not supported", p->forcemethod);
-        return r;
-    }
     if (p->forcemethod < 0 || p->forcemethod > 5) { int r = fail(h, BASTR_E_INVALID, "forcemethod %d", p->forcemethod); return r; }
     if (p->precision != BASTR_FP64 && p->precision != BASTR_FP32) { int r = fail(h, BASTR_E_INVALID, "precision"); return r; }
     const int nz = d == 3 ? p->ka : 1;
@@ -858,6 +858,7 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     // partial sums: at most one per line group of the passes that produce them
     dev_alloc(h, &h->done, kTickets * sizeof(unsigned int), st);
     dev_alloc(h, &h->pend, sizeof(double2), st);
+    dev_alloc(h, &h->rng, sizeof(unsigned long long), st);
     dev_alloc(h, &h->vg_part, (size_t)std::max(g.ny * g.nz, 1) * 8 * sizeof(double), st);
     dev_alloc(h, &h->en_part, (size_t)std::max(K * g.KY, 1) * sizeof(double), st);
     dev_alloc(h, &h->shell, (size_t)h->nshell * 4 * sizeof(double), st);
@@ -972,6 +973,11 @@ int bastr_set_counters(bastr_handle* h, int64_t nstep, double time) {
     if (!h) return BASTR_E_INVALID;
     h->nstep = nstep;
     h->time = time;
+    // the random-phase forcing stream continues from the step counter after a restart
+    const unsigned long long ctr = (unsigned long long)nstep;
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(h->rng, &ctr, sizeof(ctr), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return BASTR_OK;
 }
 
@@ -1001,7 +1007,10 @@ void decode_records(const bastr_handle* h, const double* rec, int nsteps, bastr_
             const bool vg = h->p.velgrad_every > 0 && ((n0 + i) % h->p.velgrad_every) == 0;
             for (int k = 0; k < 8; ++k) o.velgrad[k] = vg ? r[R_VG0 + k] : NAN;
             o.factor = h->p.forcemethod ? r[R_FACTOR] : NAN;
-            o.E = (h->p.forcemethod == 2 || h->p.forcemethod == 5) ? r[R_E] : NAN;
+            o.E = h->p.forcemethod >= 2 ? r[R_E] : NAN;
+            const bool rnd = h->p.forcemethod == 3 || h->p.forcemethod == 4;
+            o.energy = rnd ? r[R_ENERGY] : NAN;
+            o.Fen = rnd ? r[R_FEN] : NAN;
         }
         t = t + h->p.deltat;
     }

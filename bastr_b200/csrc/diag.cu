@@ -7,8 +7,11 @@
 //                   of each shell in fixed order -> Es, Ed shells, Esspe, Edspe, k2Edspe, kMEdspe.
 //  k_velgrad_final  velgrad_calculate2D/3D reductions and derived lengths (solution.F90:1168-1180,
 //                   1268-1280) from the x pass's per-block partials.
-//  k_force_*        forcing2D/3D methods 1, 2, 5 (solution.F90:315-378, 483-538, 554-630, 754-812).
+//  k_force_*        forcing2D/3D methods 1-5 (solution.F90:315-812).  The random phases of
+//                   methods 3 and 4 come from Philox-4x32-10 (counter-based; the reference draws
+//                   them from gfortran's random_number, so they agree in distribution only).
 #pragma once
+#include <cstdint>
 #include "solver.cuh"
 
 namespace bastr {
@@ -17,7 +20,7 @@ namespace bastr {
 enum RecSlot : int {
     R_ES = 0, R_ED, R_K2ED, R_KMED,
     R_VG0 = 4,            // 8 velocity-gradient statistics, slots 4..11
-    R_FACTOR = 12, R_E = 13, R_ENERGY = 14,
+    R_FACTOR = 12, R_E = 13, R_ENERGY = 14, R_FEN = 15,
     R_COUNT = 16
 };
 
@@ -298,13 +301,48 @@ __global__ void k_apply_pending(double2* __restrict__ U0, size_t n, const double
     }
 }
 
-// Band forcing, methods 2 and 5: the band |kk - forcek| < 1/2 is exactly the shell nint(kk) =
-// forcek.  One block enumerates it, reduces E = mean(f^2) in fixed order, then adds factor*f.
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC 2011): 10 rounds of two 32x32 -> 64-bit multiplies on a 128-bit counter, key bumped by the
+// Weyl constants between rounds.
+__host__ __device__ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// Random phase in [-pi, pi) of band mode (kx >= 0, ky, kz) at forcing call `ctr`: the mode's
+// canonical half (kx > 0, or kx = 0 with (ky, kz) > 0 lexicographically) draws it, its
+// Hermitian partner on kx = 0 takes the negative, so the force stays real.
+__device__ __forceinline__ double band_phase(int kx, int ky, int kz, unsigned long long ctr) {
+    double sgn = 1.0;
+    if (kx == 0 && (ky < 0 || (ky == 0 && kz < 0))) { ky = -ky; kz = -kz; sgn = -1.0; }
+    uint32_t c[4] = {(uint32_t)kx | ((uint32_t)(ky + 1024) << 11), (uint32_t)(kz + 1024), (uint32_t)ctr,
+                     (uint32_t)(ctr >> 32)};
+    philox4x32_10(c, 0xB5A57F01u, 0x7E5D0C2Bu);
+    const double u = ((double)c[0] + 0.5) * (1.0 / 4294967296.0);
+    return sgn * (2.0 * 3.141592653589793 * u - 3.141592653589793);
+}
+
+// Band forcing, methods 2-5: the band |kk - forcek| < 1/2 is exactly the shell nint(kk) =
+// forcek.  One block enumerates it.  Methods 2 and 5: f = the band part of u, E = mean(f^2) in
+// fixed order, then u += factor*f.  Methods 3 and 4 (solution.F90:379-482, 631-753): f has
+// unit-amplitude dilatational modes k/|k| (sin phi + i cos phi) with random phases phi; E =
+// mean(f.u), Fen = mean(f^2), energy = mean(|u|^2) (rec[R_ENERGY]); factor = (sqrt(max((target -
+// energy) Fen + E^2, 0)) - E) / Fen (method 3) or target (method 4); u += factor*f.  *rng counts
+// the forcing calls (the random stream's counter).
 template <int D, int NT>
 __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo g, int method, int forcek,
-                                                   double target, int project2d, double* __restrict__ rec) {
+                                                   double target, int project2d, double* __restrict__ rec,
+                                                   unsigned long long* rng) {
     pdl_wait();
-    __shared__ double scratch[NT];
+    __shared__ double scratch[2 * NT];
+    const bool rnd = method == 3 || method == 4;
+    const unsigned long long ctr = rnd ? *rng : 0ull;
     const int s = forcek;
     const int K = g.K;
     const long long lo = s == 0 ? 0 : (long long)s * s - s + 1;
@@ -317,7 +355,7 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
 
     // pass 1 (sum) and pass 2 (apply) walk the same modes in the same order
     for (int phase = 0; phase < 2; ++phase) {
-        double acc[1] = {0};
+        double acc[2] = {0, 0};
         double factor = 0;
         if (phase == 1) factor = rec[R_FACTOR];
         if (lo <= hi) {
@@ -347,8 +385,16 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
                         }
                         double2 f[3];
                         const size_t cst = D == 2 ? 1 : (size_t)g.ps;
-                        for (int c = 0; c < D; ++c) f[c] = U0[o + c * cst];
-                        if (D == 2 && project2d) {
+                        if (rnd) {
+                            const double phi = band_phase(kx, kyv, kzv, ctr);
+                            const double kk = sqrt((double)(rr + (long long)tt * tt));
+                            const double kv[3] = {(double)kx, (double)kyv, (double)kzv};
+                            const double2 e = make_double2(sin(phi), cos(phi));
+                            for (int c = 0; c < D; ++c) f[c] = make_double2(kv[c] / kk * e.x, kv[c] / kk * e.y);
+                        } else {
+                            for (int c = 0; c < D; ++c) f[c] = U0[o + c * cst];
+                        }
+                        if (!rnd && D == 2 && project2d) {
                             // solution.F90:498-501
                             const double kk = sqrt((double)(rr + (long long)tt * tt));
                             const double k1 = kx, k2 = kyv;
@@ -359,9 +405,16 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
                             f[1] = make_double2(ud.x * k2 / kk, ud.y * k2 / kk);
                         }
                         if (phase == 0) {
-                            double e2 = 0;
-                            for (int c = 0; c < D; ++c) e2 += f[c].x * f[c].x + f[c].y * f[c].y;
+                            double e2 = 0, fu = 0;
+                            for (int c = 0; c < D; ++c) {
+                                e2 += f[c].x * f[c].x + f[c].y * f[c].y;
+                                if (rnd) {
+                                    const double2 u = U0[o + c * cst];
+                                    fu += f[c].x * u.x + f[c].y * u.y;   // Re(f conj(u))
+                                }
+                            }
                             acc[0] += w * e2;
+                            acc[1] += w * fu;
                         } else {
                             for (int c = 0; c < D; ++c) {
                                 double2 u = U0[o + c * cst];
@@ -373,15 +426,22 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
             }
         }
         if (phase == 0) {
-            block_sum<1, NT>(acc, scratch);
+            block_sum<2, NT>(acc, scratch);
             if (threadIdx.x == 0) {
-                const double E = acc[0];
-                double fac;
+                double fac, E;
                 if (method == 2) {
+                    E = acc[0];
                     fac = sqrt(target / E) - 1.0;
-                } else {
+                } else if (method == 5) {
+                    E = acc[0];
                     const double energy = rec[R_ENERGY];
                     fac = target > energy ? sqrt((target - energy) / E + 1.0) - 1.0 : 0.0;
+                } else {
+                    const double fen = acc[0], energy = rec[R_ENERGY];
+                    E = acc[1];
+                    fac = method == 3 ? (sqrt(fmax((target - energy) * fen + E * E, 0.0)) - E) / fen : target;
+                    rec[R_FEN] = fen;
+                    *rng = ctr + 1;
                 }
                 rec[R_FACTOR] = fac;
                 rec[R_E] = E;

@@ -82,6 +82,7 @@ typedef struct bastr_step_out {
     double Esspe, Edspe, k2Edspe, kMEdspe;      /* log/stat{2,3}d_specall.dat */
     double velgrad[8];                          /* umumtheta2 umumijji u2theta dissp etamin Tay ReTay Kol */
     double factor, E;                           /* log/factor_output.dat (NaN when not written) */
+    double energy, Fen;                         /* forcing 3 and 4 also log these (else NaN) */
 } bastr_step_out;
 
 typedef struct bastr_handle bastr_handle;

@@ -14,7 +14,9 @@ complex-to-complex transforms, normalisation and quirks:
 * ``projection``             -- tool.F90:219-270
 * ``compute_ut``             -- solution.F90:816-928
 * ``rk3`` / ``cn``           -- solution.F90:172-301
-* ``forcing``                -- solution.F90:303-814 (methods 0, 1, 2, 5; 3/4 use gfortran's RNG)
+* ``forcing``                -- solution.F90:303-814 (methods 0-5; the random phases of methods
+  3/4 come from Philox-4x32-10 here and in the library, from gfortran's random_number in the
+  reference: equal in distribution, not in value)
 * ``spectra_compute``        -- solution.F90:930-1108
 * ``velgrad_calculate``      -- solution.F90:1110-1286
 * ``quantity_prepare``/``miucal`` -- solution.F90:1288-1329
@@ -172,8 +174,6 @@ class Oracle:
     def __init__(self, p: Params, u, workers: int | None = None):
         if p.timemethod not in (1, 2):
             raise ValueError("Undefined time method")  # readwrite.F90:98-104
-        if p.forcemethod in (3, 4):
-            raise NotImplementedError("forcing methods 3/4 draw from gfortran's random_number")
         self.p = p
         self.workers = workers if workers is not None else (os.cpu_count() or 1)
         self.ks = generate_wave(p)
@@ -302,6 +302,25 @@ class Oracle:
                     factor = 0.0
             self.u = [c + factor * f.real for c, f in zip(self.u, force)]
             return (factor, E)
+        if m in (3, 4):
+            # solution.F90:379-482 (2D), 631-753 (3D): unit dilatational modes k/|k| (sin phi +
+            # i cos phi) on the band; E = mean(f.u), energy = mean(|u|^2), Fen = mean(|f|^2)
+            dk = 0.5
+            kk = self.kk
+            band = ((kk - dk) < p.forcek) & ((kk + dk) > p.forcek)
+            phi = band_phases(p, self.nstep - 1, band)
+            safe = np.where(band, kk, 1.0)
+            e = np.sin(phi) + 1j * np.cos(phi)
+            force = [self.ifft(np.where(band, k / safe * e, 0.0)) for k in self.ks]
+            E = float(np.sum(sum(f.real * c for f, c in zip(force, self.u)))) / N
+            energy = float(np.sum(sum(c ** 2 for c in self.u))) / N
+            Fen = float(np.sum(sum(f.real ** 2 for f in force))) / N
+            if m == 3:
+                factor = (math.sqrt(max((p.target_energy - energy) * Fen + E * E, 0.0)) - E) / Fen
+            else:
+                factor = p.target_energy
+            self.u = [c + factor * f.real for c, f in zip(self.u, force)]
+            return (factor, E, energy, Fen)
         raise NotImplementedError(f"forcemethod {m}")
 
     # -- solution.F90:930-1108 ------------------------------------------------------------
@@ -487,3 +506,44 @@ def transfer(p: Params, u):
     sel = sh <= am
     out = [np.bincount(sh[sel], weights=t.ravel()[sel], minlength=am + 1) for t in (trans, trans1, trans2)]
     return tuple(out)
+
+
+# ---------------------------------------------------------------------------------------
+# random phases of forcing methods 3/4 (Philox-4x32-10, Salmon et al. SC 2011)
+# ---------------------------------------------------------------------------------------
+PHILOX_KEY = (0xB5A57F01, 0x7E5D0C2B)
+
+
+def philox4x32_10(c, k0, k1):
+    """Ten Philox rounds on the 4-word counter c (numpy uint32 arrays) with key (k0, k1)."""
+    c = [np.asarray(x, dtype=np.uint64) & 0xFFFFFFFF for x in c]
+    k0, k1 = np.uint64(k0), np.uint64(k1)
+    m = np.uint64(0xFFFFFFFF)
+    for _ in range(10):
+        p0 = np.uint64(0xD2511F53) * c[0]
+        p1 = np.uint64(0xCD9E8D57) * c[2]
+        hi0, lo0, hi1, lo1 = p0 >> np.uint64(32), p0 & m, p1 >> np.uint64(32), p1 & m
+        c = [(hi1 ^ c[1] ^ k0) & m, lo1, (hi0 ^ c[3] ^ k1) & m, lo0]
+        k0 = (k0 + np.uint64(0x9E3779B9)) & m
+        k1 = (k1 + np.uint64(0xBB67AE85)) & m
+    return [x.astype(np.uint32) for x in c]
+
+
+def band_phases(p: Params, ctr: int, band: np.ndarray) -> np.ndarray:
+    """Phase of every grid mode for forcing call ctr (zero off the band): each mode's canonical
+    half (kx > 0, or kx = 0 with (ky, kz) > 0) draws phi = 2 pi (u - 1/2) from Philox of
+    (kx | (ky+1024) << 11, kz + 1024, ctr lo, ctr hi); the other half takes -phi(-k)."""
+    ks = generate_wave(p)
+    kx = ks[0].astype(np.int64)
+    ky = ks[1].astype(np.int64)
+    kz = ks[2].astype(np.int64) if p.ndims == 3 else np.zeros_like(kx)
+    neg = (kx < 0) | ((kx == 0) & ((ky < 0) | ((ky == 0) & (kz < 0))))
+    sgn = np.where(neg, -1.0, 1.0)
+    ax, ay, az = np.where(neg, -kx, kx), np.where(neg, -ky, ky), np.where(neg, -kz, kz)
+    c0 = (ax | ((ay + 1024) << 11)).astype(np.uint64)
+    c1 = (az + 1024).astype(np.uint64)
+    c2 = np.full_like(c0, ctr & 0xFFFFFFFF)
+    c3 = np.full_like(c0, (ctr >> 32) & 0xFFFFFFFF)
+    out = philox4x32_10([c0, c1, c2, c3], *PHILOX_KEY)
+    u = (out[0].astype(np.float64) + 0.5) / 4294967296.0
+    return np.where(band, sgn * (2.0 * np.pi * u - np.pi), 0.0)

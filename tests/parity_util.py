@@ -59,6 +59,9 @@ def compare(ref, gpu, velgrad: bool = True):
         err["factor"] = rel_l2([r.factor for r in grec], [r.forcing[0] for r in rrec])
         if len(rrec[0].forcing) > 1:
             err["E"] = rel_l2([r.E for r in grec], [r.forcing[1] for r in rrec])
+        if len(rrec[0].forcing) > 3:   # random-phase forcing also logs energy and Fen
+            err["energy"] = rel_l2([r.energy for r in grec], [r.forcing[2] for r in rrec])
+            err["Fen"] = rel_l2([r.Fen for r in grec], [r.forcing[3] for r in rrec])
     # every spectrum shell: relative L2 over the shell vector, worst over steps
     am = rsh.shape[-1]
     es = max(rel_l2(gsh[i, 0, :am], rsh[i, 0]) for i in range(len(rsh)))

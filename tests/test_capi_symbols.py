@@ -42,7 +42,7 @@ def test_create_rejects_bad_parameters_without_gpu(gpu_lib):
     lib.bastr_destroy.argtypes = [ctypes.c_void_p]
     cases = [
         (dict(ia=64, ja=64, ka=0, timemethod=3), -1, "time method"),
-        (dict(ia=64, ja=64, ka=0, forcemethod=3), -2, "random-phase"),
+        (dict(ia=64, ja=64, ka=0, forcemethod=6), -1, "forcemethod 6"),
         (dict(ia=96, ja=96, ka=0), -2, "power of two"),
         (dict(ia=64, ja=16, ka=0), -2, "2*floor"),
         (dict(ia=1024, ja=1024, ka=1024), -2, "3D extents"),

@@ -149,3 +149,18 @@ def test_transfer_spectra_match_oracle(gpu_lib, dims):
     ref = transfer(p, uf)
     for g, r in zip(got, ref):
         assert rel_l2(g[1:], r[1:]) <= 1e-12, (g[1:6], r[1:6])
+
+
+@pytest.mark.parametrize("dims,method", [((64, 64, 0), 3), ((64, 64, 0), 4), ((16, 16, 16), 3), ((16, 16, 16), 4)],
+                         ids=["2d_m3", "2d_m4", "3d_m3", "3d_m4"])
+def test_random_phase_forcing_matches_oracle(gpu_lib, dims, method):
+    """Forcing methods 3 and 4 (random phases from the shared Philox stream): velocity, spectra,
+    factor, E, energy and Fen of 1 and of 10 steps."""
+    ia, ja, ka = dims
+    target = 1.0 if method == 3 else 1e-3
+    p = make_params(ia, ja, ka, reynolds=1000.0, deltat=1e-3, forcemethod=method, forcek=3,
+                    target_energy=target, kmax=100)
+    u = field(ia, ja, ka, k0=3.0, seed=6)
+    for n, tol in ((1, 1e-12), (10, 1e-9)):
+        err = compare(run_oracle(p, u, n), run_gpu(p, u, n, "fp64"))
+        _check(err, tol)

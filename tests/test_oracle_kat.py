@@ -183,3 +183,33 @@ def test_listwrite_format():
     assert fortran_e20_13(1.5e-120) == " 0.1500000000000-119"
     line = listwrite_line(3, 3e-4, 1.0, 2.0)
     assert line == "                    3  0.3000000000000E-03  0.1000000000000E+01  0.2000000000000E+01"
+
+
+def test_philox_known_answers():
+    """Philox-4x32-10 against the published known-answer vectors (Salmon et al. 2011)."""
+    import numpy as np
+    from oracle.bastr_oracle import philox4x32_10
+    cases = [((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+             ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+             ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+              (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1))]
+    for c, k, want in cases:
+        out = philox4x32_10([np.array([x], np.uint64) for x in c], *k)
+        assert tuple(int(o[0]) for o in out) == want
+
+
+def test_random_phase_force_is_real_and_in_band():
+    import numpy as np
+    from oracle.bastr_oracle import Params, band_phases, generate_wave
+    for p in (Params(ia=32, ja=32, ka=0, forcek=4), Params(ia=16, ja=16, ka=16, forcek=3)):
+        ks = generate_wave(p)
+        kk = np.sqrt(sum(k * k for k in ks))
+        band = np.abs(kk - p.forcek) < 0.5
+        phi = band_phases(p, 7, band)
+        safe = np.where(band, kk, 1.0)
+        e = np.sin(phi) + 1j * np.cos(phi)
+        for k in ks:
+            f = np.fft.ifftn(np.where(band, k / safe * e, 0.0))
+            assert np.max(np.abs(f.imag)) < 1e-14 * max(1.0, np.max(np.abs(f.real)))
+        assert np.all(phi[~band] == 0) and np.all(np.abs(phi[band]) <= np.pi)
+        assert not np.array_equal(band_phases(p, 8, band), phi)   # a new draw every call
