@@ -43,7 +43,7 @@ EXPORTED = [
     "bastr_ensemble_get_state", "bastr_ensemble_step", "bastr_ensemble_set_plan", "bastr_ensemble_get_plan",
     "bastr_ensemble_tune", "bastr_ensemble_last_error",
     "bastr_net_nparams", "bastr_net_grad_blocks", "bastr_net_forward", "bastr_net_grad", "bastr_net_adam",
-    "bastr_closure_apply", "bastr_transfer",
+    "bastr_closure_apply", "bastr_transfer", "bastr_hitgen",
 ]
 BASTR_E_TOO_LARGE = -6
 
@@ -126,6 +126,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_net_adam.argtypes = [P, P, P, P, P, C.c_int32, C.c_float, C.c_float, C.c_float, C.c_float, P]
     lib.bastr_closure_apply.argtypes = [P, P, C.c_float, C.c_double]
     lib.bastr_transfer.argtypes = [P, D, D, D]
+    lib.bastr_hitgen.argtypes = [P, C.c_int32, C.c_uint64, D, D, D, D, D]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -284,6 +285,20 @@ class BastrGPU:
         t, t1, t2 = (np.empty(n) for _ in range(3))
         self._check(self.lib.bastr_transfer(self.h, _dptr(t), _dptr(t1), _dptr(t2)))
         return t, t1, t2
+
+    def hitgen(self, variant: int = 0, seed: int = 0):
+        """Bastrpp's initial-field generators (hitgen2d / hitgen3d = variant 0, hitgen2dbis =
+        variant 1) on this handle's grid, forcek and target_energy.  Returns (fields, angle,
+        stats): the physical u1, u2[, u3], the random_angle field and a dict of energy (before
+        scaling), factor, alpha, residual, QX, QY, QZ, QW.  The state is not changed."""
+        out = [np.empty(self.shape, dtype=np.float64) for _ in range(self.ndims)]
+        angle = np.empty(self.shape, dtype=np.float64)
+        st = np.empty(8, dtype=np.float64)
+        u3 = out[2] if self.ndims == 3 else None
+        self._check(self.lib.bastr_hitgen(self.h, variant, seed & 0xFFFFFFFFFFFFFFFF, _dptr(out[0]), _dptr(out[1]),
+                                          _dptr(u3) if u3 is not None else None, _dptr(angle), _dptr(st)))
+        names = ("energy", "factor", "alpha", "residual", "QX", "QY", "QZ", "QW")
+        return out, angle, dict(zip(names, st.tolist()))
 
     def closure_apply(self, net, scale: float, dt: float):
         """One closure sub-step u <- u - dt * scale * net(u) on this (3D) solver's state; `net` is

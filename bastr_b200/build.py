@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbastr_gpu.so")
 SOURCES = ["capi.cu", "noalloc.cu"]
-DEPS = ["capi.cu", "pass2d.cu", "pass3d.cu", "diag.cu", "ensemble.cu", "fullfft.cu", "closure.cu", "transfer.cu", "noalloc.cu", "fft_engine.cuh", "regfft.cuh",
+DEPS = ["capi.cu", "pass2d.cu", "pass3d.cu", "diag.cu", "ensemble.cu", "fullfft.cu", "closure.cu", "transfer.cu", "hitgen.cu", "noalloc.cu", "fft_engine.cuh", "regfft.cuh",
         "solver.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

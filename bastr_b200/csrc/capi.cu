@@ -32,6 +32,7 @@
 #include "fullfft.cu"
 #include "closure.cu"
 #include "transfer.cu"
+#include "hitgen.cu"
 
 using namespace bastr;
 
@@ -76,6 +77,7 @@ struct bastr_handle {
     float* closure_buf = nullptr;  // 3D closure: tau_hat [3][n] (allocated on first use)
     double2* tr_buf = nullptr;     // transfer spectra: full complex grids (allocated on first use)
     double* tr_modes = nullptr;    // transfer spectra: per-mode values, item partials, shell sums
+    double* hg_part = nullptr;     // initial-field generators: per-block partial sums
     double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
     unsigned long long* rng = nullptr;  // forcing calls so far: counter of the random-phase stream
     bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
@@ -728,7 +730,7 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
 }
 
 void free_all(bastr_handle* h) {
-    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->rng, h->closure_buf, h->tr_buf, h->tr_modes,
+    void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->rng, h->closure_buf, h->tr_buf, h->tr_modes, h->hg_part,
                     h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
                     h->sp_item_part};
     for (void* q : ptrs)
@@ -1292,6 +1294,85 @@ int bastr_transfer(bastr_handle* h, double* T, double* T1, double* T2) {
     for (int k = 0; k < 3; ++k) {
         if (!dst[k]) continue;
         for (int s2 = 0; s2 <= h->allkmax; ++s2) dst[k][s2] = s2 < h->nshell ? buf[(size_t)k * h->nshell + s2] : 0.0;
+    }
+    return BASTR_OK;
+}
+
+// Bastrpp's initial-field generators (hitgen.cu).  Work arrays: full complex grids of the
+// transfer buffer (R, field A, field B, angle) and the physical-field buffer for the result.
+int bastr_hitgen(bastr_handle* h, int32_t variant, uint64_t seed, double* u1, double* u2, double* u3,
+                 double* angle, double* stats) {
+    if (!h) return BASTR_E_INVALID;
+    if (variant != 0 && variant != 1) return fail(h, BASTR_E_INVALID, "hitgen variant must be 0 or 1");
+    const Geo& g = h->g;
+    const int D = g.d;
+    if (variant == 1 && D != 2) return fail(h, BASTR_E_UNSUPPORTED, "hitgen2dbis is two-dimensional");
+    if (!(h->p.forcek > 0)) return fail(h, BASTR_E_INVALID, "hitgen needs forcek > 0");
+    CK(cudaSetDevice(h->device));
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    const size_t narr = (size_t)(D + D * D + D + D + D * D);   // the transfer buffer's size
+    constexpr int NB = 148 * 4, NT = 256;
+    if (!h->tr_buf) CK(cudaMalloc(&h->tr_buf, narr * n * sizeof(double2)));
+    if (!h->hg_part) CK(cudaMalloc(&h->hg_part, (size_t)NB * 4 * sizeof(double)));
+    const bool bis = variant == 1;
+    double2* R = h->tr_buf;
+    double2* A = R + n;
+    double2* B = A + 3 * n;
+    double* ang = reinterpret_cast<double*>(bis ? B + 3 * n : A + 3 * n);
+    const int gs = 148 * 8;
+    std::vector<double> part((size_t)NB * 4);
+    auto sums = [&](const double2* X, const double2* Y, double alpha, int mode, double out[4]) -> int {
+        k_hg_sums<NT><<<NB, NT, 0, h->stream>>>(X, Y, alpha, D, n, mode, h->hg_part);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(part.data(), h->hg_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int i = 0; i < 4; ++i) out[i] = 0.0;
+        for (int b = 0; b < NB; ++b)
+            for (int i = 0; i < 4; ++i) out[i] += part[(size_t)b * 4 + i];
+        return BASTR_OK;
+    };
+    // one draw: uniform field -> R -> modes of F -> physical (real parts used)
+    auto draw = [&](int d, double2* F) -> int {
+        k_hg_uniform<<<gs, 256, 0, h->stream>>>(R, ang, n, d, (unsigned long long)seed);
+        CK(cudaGetLastError());
+        for (int a = 0; a < D; ++a) CK(full_axis<false>(h, R, a, a == D - 1 ? g.inv_n : 1.0));
+        if (D == 2) k_hg_modes<2><<<gs, 256, 0, h->stream>>>(R, F, ang, g, (double)h->p.forcek, bis, bis);
+        else k_hg_modes<3><<<gs, 256, 0, h->stream>>>(R, F, ang, g, (double)h->p.forcek, 0, 0);
+        CK(cudaGetLastError());
+        const int nf = bis ? D + 1 : D;
+        for (int c = 0; c < nf; ++c)
+            for (int a = 0; a < D; ++a) CK(full_axis<true>(h, F + (size_t)c * n, a, 1.0));
+        return BASTR_OK;
+    };
+    int rc = draw(0, A);
+    if (rc != BASTR_OK) return rc;
+    double alpha = 0.0, check = std::nan(""), q[4] = {0, 0, 0, 0};
+    const double2* Bc = nullptr;
+    if (bis) {
+        rc = draw(1, B);
+        if (rc != BASTR_OK) return rc;
+        rc = sums(A, B, 0.0, 1, q);
+        if (rc != BASTR_OK) return rc;
+        for (int i = 0; i < 4; ++i) q[i] *= g.inv_n;
+        alpha = hitgen_cubic_root(q[0], q[1], q[2], q[3]);
+        check = q[0] + alpha * q[1] + alpha * alpha * q[2] + alpha * alpha * alpha * q[3];
+        Bc = B;
+    }
+    double e[4];
+    rc = sums(A, Bc, alpha, 0, e);
+    if (rc != BASTR_OK) return rc;
+    const double energy = e[0] / ((double)g.nx * g.ny * g.nz);
+    const double factor = std::sqrt(h->p.target_energy / energy);
+    k_hg_finish<<<gs, 256, 0, h->stream>>>(A, Bc, alpha, factor, D, n, h->phys);
+    CK(cudaGetLastError());
+    double* dst[3] = {u1, u2, u3};
+    for (int c = 0; c < D; ++c)
+        if (dst[c]) CK(cudaMemcpyAsync(dst[c], h->phys + (size_t)c * n, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (angle) CK(cudaMemcpyAsync(angle, ang, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (stats) {
+        const double v[8] = {energy, factor, bis ? alpha : std::nan(""), check, q[0], q[1], q[2], q[3]};
+        for (int i = 0; i < 8; ++i) stats[i] = v[i];
     }
     return BASTR_OK;
 }

@@ -1,17 +1,12 @@
-// Shared-memory Stockham FFT engine for sm_100a.
+// Complex arithmetic and register DFTs shared by the transforms of sm_100a passes.
 //
-// A thread block transforms U independent complex sequences ("units") of length N that sit
-// in shared memory.  Each stage of radix R reads R elements per butterfly at stride N/R,
-// applies the twiddles, runs a register-resident DFT-R and writes the results in Stockham
-// autosort order, so the final stage leaves natural order without a bit-reversal pass.
-// Every thread holds all of its butterflies of one stage in registers between the read and
-// the write phase, which lets the stage run in place.
+// cplx<T> is float2 / double2; the single-precision add, subtract and scale use Blackwell's
+// packed FP32x2 instructions.  dft2/4/8/16 are in-register DFTs in natural order (the radix
+// kernels of the Stockham transforms in regfft.cuh); rot4 is the quarter turn of the
+// transform's sign.
 //
-// Shared-memory addresses are padded by one element every 16 (pidx) so that the stride-R
-// writes of the first stages do not collide on the same banks.
-//
-// Twiddles come from a table tw[m] = exp(-2*pi*i*m/N) generated on the host in extended
-// precision and rounded once to the compute type; the inverse direction conjugates them.
+// Shared-memory addresses of staged lines are padded by one element every 16 (pidx) so that
+// strided accesses do not collide on the same banks.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -151,86 +146,6 @@ template <typename T, bool INV, int R> __device__ __forceinline__ void dftR(cplx
     else if constexpr (R == 4) dft4<T, INV>(v);
     else if constexpr (R == 8) dft8<T, INV>(v);
     else dft16<T, INV>(v);
-}
-
-// Radix of the next stage given the remaining factor REM = N / P.
-__host__ __device__ constexpr int next_radix(int rem) {
-    return (rem % 16 == 0 && rem != 32) ? 16 : (rem % 8 == 0) ? 8 : (rem % 4 == 0) ? 4 : 2;
-}
-
-// ---------------------------------------------------------------------------------------
-// One Stockham stage over U units.  Units come in groups of G: unit u starts at
-// s + (u/G)*GS + (u%G)*USTR (padded addressing inside a unit).
-// ---------------------------------------------------------------------------------------
-template <int G, int GS, int USTR> __device__ __forceinline__ int unit_off(int u) {
-    if constexpr (G == 1) return u * GS;
-    else return (u / G) * GS + (u % G) * USTR;
-}
-
-template <typename T, int N, int R, int P, int U, int USTR, int NT, bool INV, int G, int GS>
-__device__ __forceinline__ void fft_stage(cplx<T>* __restrict__ s, const cplx<T>* __restrict__ tw) {
-    constexpr int NB = N / R;          // butterflies per unit
-    constexpr int TOT = U * NB;
-    constexpr int PER = (TOT + NT - 1) / NT;
-    constexpr int TWS = N / (P * R);   // twiddle table stride
-    cplx<T> v[PER][R];
-    const int tid = threadIdx.x;
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int b = tid + q * NT;
-        if ((TOT % NT == 0) || b < TOT) {
-            const int u = b / NB, i = b - u * NB;
-            const int k = i & (P - 1);
-            cplx<T>* src = s + unit_off<G, GS, USTR>(u);
-#pragma unroll
-            for (int j = 0; j < R; ++j) v[q][j] = src[pidx(i + j * NB)];
-            if constexpr (P > 1) {
-#pragma unroll
-                for (int j = 1; j < R; ++j) {
-                    cplx<T> w = tw[j * k * TWS];
-                    if (INV) w.y = -w.y;
-                    v[q][j] = cmul<T>(v[q][j], w);
-                }
-            }
-            dftR<T, INV, R>(v[q]);
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int b = tid + q * NT;
-        if ((TOT % NT == 0) || b < TOT) {
-            const int u = b / NB, i = b - u * NB;
-            const int k = i & (P - 1);
-            cplx<T>* dst = s + unit_off<G, GS, USTR>(u);
-            const int base = (i - k) * R + k;
-#pragma unroll
-            for (int j = 0; j < R; ++j) dst[pidx(base + j * P)] = v[q][j];
-        }
-    }
-    __syncthreads();
-}
-
-// Full transform: all stages.  Unnormalised in both directions; forward uses exp(-i...).
-// The caller must __syncthreads() after filling the units.
-template <typename T, int N, int U, int USTR, int NT, bool INV, int G = U, int GS = U * USTR, int P = 1>
-__device__ __forceinline__ void fft_run(cplx<T>* __restrict__ s, const cplx<T>* __restrict__ tw) {
-    if constexpr (P < N) {
-        constexpr int R = next_radix(N / P);
-        fft_stage<T, N, R, P, U, USTR, NT, INV, G, GS>(s, tw);
-        fft_run<T, N, U, USTR, NT, INV, G, GS, P * R>(s, tw);
-    }
-}
-
-// Threads per block for U units of length N: each thread holds at most EPT complex values
-// per stage (16 doubles-complex = 64 registers, 32 floats-complex = 64 registers).
-template <typename T> __host__ __device__ constexpr int elems_per_thread() { return sizeof(T) == 8 ? 16 : 32; }
-template <typename T, int UN> __host__ __device__ constexpr int pick_threads() {
-    int nt = (UN + elems_per_thread<T>() - 1) / elems_per_thread<T>();
-    nt = ((nt + 31) / 32) * 32;
-    if (nt < 64) nt = 64;
-    if (nt > 1024) nt = 1024;
-    return nt;
 }
 
 }  // namespace bastr

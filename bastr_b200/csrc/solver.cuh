@@ -26,9 +26,8 @@ struct Geo {
     double inv_n;       // 1 / (nx*ny*nz)
 };
 
-// truncated index -> wavenumber, and -> position in a length-n transform
+// truncated index -> wavenumber
 __device__ __forceinline__ int trunc_k(int i, int K, int KT) { return i < K ? i : i - KT; }
-__device__ __forceinline__ int trunc_pos(int i, int K, int KT, int n) { return i < K ? i : i + (n - KT); }
 // position in a length-n transform -> truncated index, or -1 outside the kept set
 __device__ __forceinline__ int pos_trunc(int p, int K, int KT, int n) {
     return p < K ? p : (p > n - K ? p - (n - KT) : -1);
@@ -140,11 +139,6 @@ struct StageIO {
     double* energy_part; // per-block sum of w*|u0_new|^2 (RK3 / CN_LAST), or null
 };
 
-template <typename T>
-__device__ __forceinline__ double2 ld_stage(const StageIO<T>& io, size_t o, bool from_u0) {
-    return from_u0 ? io.u0[o] : cvt<cplx<T>, double2>(io.us[o]);
-}
-__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 dscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 
 // State values one mode's epilogue reads: the FP64 state a = u0, the stage input s (us; equal to
@@ -292,12 +286,6 @@ __device__ __forceinline__ void stage_line(void* smem_dst, const void* gmem_src,
         const int n8 = bytes >> 3;
         for (int i = threadIdx.x; i < n8; i += blockDim.x) cp_async8(d + 8 * i, s + 8 * i);
     }
-}
-
-// Lines (or rows) per block so that one block holds about 48 KB of transform data; a power of 2.
-template <typename T> __host__ __device__ constexpr int target_elems() { return sizeof(T) == 8 ? 3072 : 6144; }
-template <typename T, int N, int F> __host__ __device__ constexpr int lines_per_block() {
-    return pow2_floor(target_elems<T>() / (F * N));
 }
 
 }  // namespace bastr

@@ -191,6 +191,43 @@ def kernel_roofline(s, nsteps, peak, peak_kind, wl, prec):
             "share_of_step": round(top["total_ms"] / total, 4)}, shares
 
 
+def fp32_accuracy(device, steps={"2d2048": 100, "3d256": 20}):
+    """The FP32 form's error against the FP64 form on the GPU, per result, at the measured sizes:
+    both forms step the same seeded field; relative L2 of the velocity, of each per-step scalar
+    sequence and of every spectrum shell (worst step).  Untimed."""
+    import numpy as np
+    out = {}
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+        nb = np.linalg.norm(b)
+        return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+    for wl, n in steps.items():
+        runs = {}
+        for prec in ("fp64", "fp32"):
+            s = make_solver(wl, prec, device)
+            s.set_state(initial_field(wl))
+            recs, sh = s.step(n, shells=True)
+            runs[prec] = (recs, sh, np.stack(s.get_state()))
+            s.close()
+        (r64, s64, u64), (r32, s32, u32) = runs["fp64"], runs["fp32"]
+        e = {"steps": n, "velocity": rel(u32, u64)}
+        for name in ("Esspe", "Edspe", "k2Edspe", "kMEdspe", "factor"):
+            e[name] = rel([getattr(r, name) for r in r32], [getattr(r, name) for r in r64])
+        if math.isfinite(r64[0].E):
+            e["E"] = rel([r.E for r in r32], [r.E for r in r64])
+        vg = ("umumtheta2", "umumijji", "u2theta", "dissp", "eta_min", "Tay", "ReTay", "Kol")
+        for i, name in enumerate(vg):
+            e[name] = rel([r.velgrad[i] for r in r32], [r.velgrad[i] for r in r64])
+        e["Es_shells"] = max(rel(s32[i, 0], s64[i, 0]) for i in range(n))
+        e["Ed_shells"] = max(rel(s32[i, 1], s64[i, 1]) for i in range(n))
+        e = {k: (float(f"{v:.3g}") if isinstance(v, float) else v) for k, v in e.items()}
+        e["max_except_eta_min"] = max(v for k, v in e.items() if k not in ("steps", "eta_min"))
+        out[wl] = e
+    return out
+
+
 def ensemble_measure(device, steps=30, tune=True):
     """The standard ensemble (96 realizations: 32 each at 256^2, 512^2, 1024^2, seeds 0-95, band
     forcing with forcek in {3..8}, target in [0.05, 0.1], FP32), advanced as one CUDA graph per
@@ -364,6 +401,7 @@ def ours(args):
     ens = (ensemble_measure(device) if (rank == 0 and n_gpus == 1 and not args.no_variants and not args.no_ensemble)
            else None)
     base = cpu_baseline(wl) if (rank == 0 and n_gpus == 1 and not args.no_cpu) else None
+    acc = fp32_accuracy(device) if (rank == 0 and n_gpus == 1 and not args.no_variants) else None
     if dist_ctx:
         dist_ctx.barrier()
         dist_ctx.close()
@@ -385,6 +423,7 @@ def ours(args):
         "survey_roofline_frac": round(survey_bytes(w, prec) / (ms / args.steps * 1e-3) / (peak * 1e9), 4),
         "roofline": roof, "kernel_shares": shares, "variants": variants, "ensemble": ens,
         "cpu_baseline": base, "e2e": e2e,
+        "fp32_vs_fp64_rel_l2": acc,
         "gpu_launches": int(info["launches_per_step"] * args.steps),
         "clocks": clocks,
     }

@@ -23,6 +23,8 @@
  * bastr_fft                   fft2d/fft3d/ifft2d/ifft3d (fftwlink.F90:324-368), in place on a
  *                             full complex(8) grid, for Bastrpp-style callers
  * bastr_destroy               deallocation (fftwlink.F90:469-490)
+ * bastr_transfer              Bastrpp transfer2d/transfer3d (Bastrpp.F90:174-305, 418-599)
+ * bastr_hitgen                Bastrpp hitgen2d/hitgen2dbis/hitgen3d (Bastrpp.F90:601-1005)
  * bastr_profile, bastr_info,  no reference counterpart: per-kernel timing and introspection
  *   bastr_step_async/records,  for measurement; asynchronous stepping and stream control
  *   bastr_set_stream, bastr_sync
@@ -114,6 +116,19 @@ BASTR_API int bastr_spectra(bastr_handle* h, double* kn, double* Es, double* Ed,
  * u_i div(u) part) per shell nint(|k|) = 0..allkmax (host arrays of allkmax+1; any may be NULL).
  * Allocates its full-grid work buffers on the first call (about (2d + 2d^2) complex grids). */
 BASTR_API int bastr_transfer(bastr_handle* h, double* T, double* T1, double* T2);
+
+/* Initial-field generators of Bastrpp: variant 0 = hitgen2d / hitgen3d (create_initial_field_2d
+ * Bastrpp.F90:601-696, create_initial_field_3d :698-808, by the handle's dimension), variant 1 =
+ * hitgen2dbis (create_initial_field_2d_bis :810-1005, 2D only).  A dilatational field with the
+ * generators' spectrum (the handle's forcek) and random phases, scaled to mean(|u|^2) = the
+ * handle's target_energy.  The phases are atan2 of the FFT of a uniform (0,1) field drawn from
+ * Philox-4x32-10 keyed by `seed` (not gfortran's random_number).  Host outputs, x fastest (any may
+ * be NULL): u1, u2[, u3] and random_angle (the phase of every mode; the uniform value at k = 0).
+ * stats[8] (may be NULL): energy before scaling, factor, alpha (NaN for variant 0), the cubic's
+ * residual at alpha, QX, QY, QZ, QW.  The handle's state is not changed; pass the result to
+ * bastr_set_state to start from it.  Uses the work buffers of bastr_transfer. */
+BASTR_API int bastr_hitgen(bastr_handle* h, int32_t variant, uint64_t seed, double* u1, double* u2, double* u3,
+                           double* angle, double* stats);
 
 /* In-place c2c transform of a full complex(8) grid (interleaved re,im; x fastest):
  * dir = -1 forward scaled by 1/N (fft2d/fft3d), dir = +1 backward unscaled (ifft2d/ifft3d). */

@@ -23,6 +23,9 @@ complex-to-complex transforms, normalisation and quirks:
 * ``readinput`` derivations  -- readwrite.F90:69-83 (ndims, allkmax)
 * ``mainloop``               -- solution.F90:20-170
 * ``listwrite`` format       -- utility.F90:87-164 ``(1X,I20,n(1X,E20.13E2))``
+* ``transfer``               -- Bastrpp.F90:174-305, 418-599 (transfer2d / transfer3d)
+* ``hitgen``                 -- Bastrpp.F90:601-1005 (hitgen2d / hitgen3d / hitgen2dbis; the uniform
+  numbers come from Philox-4x32-10 here and in the library, from random_number in the reference)
 
 Layout: fields are NumPy arrays in C order ``(ny, nx)`` for 2D and ``(nz, ny, nx)`` for 3D,
 i.e. the same bytes as the reference's Fortran ``u(1:im,1:jm[,1:km])`` with x fastest.
@@ -547,3 +550,91 @@ def band_phases(p: Params, ctr: int, band: np.ndarray) -> np.ndarray:
     out = philox4x32_10([c0, c1, c2, c3], *PHILOX_KEY)
     u = (out[0].astype(np.float64) + 0.5) / 4294967296.0
     return np.where(band, sgn * (2.0 * np.pi * u - np.pi), 0.0)
+
+
+# ---------------------------------------------------------------------------------------
+# initial-field generators of Bastrpp (hitgen2d / hitgen2dbis / hitgen3d)
+# ---------------------------------------------------------------------------------------
+HITGEN_TAG = 0x48475431
+
+
+def hitgen_uniform(p: Params, draw: int, seed: int) -> np.ndarray:
+    """Uniform (0,1) field (53-bit) for draw `draw`: Philox-4x32-10 keyed by the 64-bit seed on the
+    counter (point index lo, hi, draw, tag), point index x fastest.  Stands in for gfortran's
+    random_number(random_angle) (Bastrpp.F90:637, 737, 849, 889)."""
+    idx = np.arange(p.npts, dtype=np.uint64)
+    c = [idx & np.uint64(0xFFFFFFFF), idx >> np.uint64(32), np.full_like(idx, draw), np.full_like(idx, HITGEN_TAG)]
+    out = philox4x32_10(c, seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
+    x = (out[0].astype(np.uint64) << np.uint64(32)) | out[1].astype(np.uint64)
+    u = ((x >> np.uint64(11)).astype(np.float64) + 0.5) * (1.0 / 9007199254740992.0)
+    return u.reshape(p.shape)
+
+
+def hitgen_modes(p: Params, r: np.ndarray, bis: bool):
+    """One draw of the generators (Bastrpp.F90:641-666 2D, 741-771 3D, 853-876 / 893-916 bis):
+    theta = atan2 of FFT(r), u^_c = var2 k_c/|k| (sin theta + i cos theta); for bis also
+    theta^ = i (kx u^_1 + ky u^_2).  Returns (u^ list, theta^ or None, random_angle)."""
+    d = p.ndims
+    n = p.npts
+    ks = generate_wave(p)
+    R = np.fft.fftn(r.astype(np.complex128)) / n
+    kk = np.sqrt(sum(k * k for k in ks))
+    zero = kk == 0
+    kks = np.where(zero, 1.0, kk)
+    fk = float(p.forcek)
+    if bis:
+        var1 = kks ** 4 * np.exp(-2.0 * (kks / fk) ** 2)
+    else:
+        var1 = np.where(kks >= fk, kks ** 4 * np.exp(-2.0 * (kks / fk) ** 2), fk ** 6 / kks ** 2 * np.exp(-2.0))
+    var2 = np.sqrt(var1 / 2.0 / np.pi / kks) if d == 2 else np.sqrt(var1 / 4.0 / np.pi / kks ** 2)
+    th = np.arctan2(R.imag, R.real)
+    angle = np.where(zero, r, th)
+    ph = np.sin(th) + 1j * np.cos(th)
+    us = [np.where(zero, 0.0, var2 * ks[c] / kks * ph) for c in range(d)]
+    thspe = (1j * (ks[0] * us[0] + ks[1] * us[1])) if bis else None
+    return us, thspe, angle
+
+
+def hitgen_alpha(QX, QY, QZ, QW):
+    """The real root of QX + QY a + QZ a^2 + QW a^3 = 0 the reference takes (Bastrpp.F90:951-973)."""
+    QP = QY / QW - (1.0 / 3.0) * (QZ / QW) ** 2
+    QQ = 2.0 / 27.0 * (QZ / QW) ** 3 - (1.0 / 3.0) * (QZ * QY) / QW ** 2 + QX / QW
+    QDELTA = (QQ / 2.0) ** 2 + (QP / 3.0) ** 3
+    if QDELTA >= 0.0:
+        t1 = -QQ / 2.0 + math.sqrt(QDELTA)
+        t2 = -QQ / 2.0 - math.sqrt(QDELTA)
+        return math.copysign(abs(t1) ** (1.0 / 3.0), t1) + math.copysign(abs(t2) ** (1.0 / 3.0), t2) - QZ / (3.0 * QW)
+    return 2.0 * math.sqrt(-QP / 3.0) * math.cos((1.0 / 3.0) * math.acos(3.0 * QQ / (2.0 * QP) * math.sqrt(-3.0 / QP))) \
+        - QZ / (3.0 * QW)
+
+
+def hitgen(p: Params, variant: int, seed: int):
+    """create_initial_field_2d / _3d (variant 0; Bastrpp.F90:601-808) and create_initial_field_2d_bis
+    (variant 1; :810-1005) with p.forcek and p.target_energy.  Returns (u list, random_angle,
+    stats dict: energy before scaling, factor, alpha, residual, QX..QW)."""
+    n = p.npts
+    bwd = lambda a: np.fft.ifftn(a) * n       # noqa: E731  ifft2d/ifft3d (fftwlink.F90:349-368)
+    us, th, angle = hitgen_modes(p, hitgen_uniform(p, 0, seed), variant == 1)
+    uA = [bwd(c).real for c in us]
+    st = {"alpha": float("nan"), "residual": float("nan"), "QX": 0.0, "QY": 0.0, "QZ": 0.0, "QW": 0.0}
+    if variant == 1:
+        thA = bwd(th).real
+        us, th, angle = hitgen_modes(p, hitgen_uniform(p, 1, seed), True)
+        uB = [bwd(c).real for c in us]
+        thB = bwd(th).real
+        aa = uA[0] ** 2 + uA[1] ** 2
+        bb = uB[0] ** 2 + uB[1] ** 2
+        ab = uB[0] * uA[0] + uB[1] * uA[1]
+        QX = float(np.sum(aa * thA)) / n
+        QY = float(np.sum(2 * ab * thA + aa * thB)) / n
+        QZ = float(np.sum(2 * ab * thB + bb * thA)) / n
+        QW = float(np.sum(bb * thB)) / n
+        a = hitgen_alpha(QX, QY, QZ, QW)
+        st.update(alpha=a, residual=QX + a * QY + a * a * QZ + a ** 3 * QW, QX=QX, QY=QY, QZ=QZ, QW=QW)
+        u = [uA[c] + a * uB[c] for c in range(2)]
+    else:
+        u = uA
+    energy = float(sum(np.sum(c * c) for c in u)) / n
+    factor = math.sqrt(p.target_energy / energy)
+    st.update(energy=energy, factor=factor)
+    return [c * factor for c in u], angle, st

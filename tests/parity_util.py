@@ -73,5 +73,27 @@ def compare(ref, gpu, velgrad: bool = True):
     return err
 
 
+def compare_gpu_runs(ref, other, velgrad: bool = True):
+    """Relative errors of one GPU run (`other`) against another (`ref`, e.g. the FP64 form):
+    velocity, each per-step scalar, forcing factor and E, every spectrum shell (worst step)."""
+    rrec, rsh, ru = ref
+    grec, gsh, gu = other
+    err = {"velocity": rel_l2(np.stack(gu), np.stack(ru))}
+    names = ["Esspe", "Edspe", "k2Edspe", "kMEdspe", "factor"]
+    if math.isfinite(rrec[0].E):   # forcing methods that log E (NaN in the record otherwise)
+        names.append("E")
+    for name in names:
+        err[name] = rel_l2([getattr(r, name) for r in grec], [getattr(r, name) for r in rrec])
+    if velgrad:
+        vg = ("umumtheta2", "umumijji", "u2theta", "dissp", "eta_min", "Tay", "ReTay", "Kol")
+        for i, name in enumerate(vg):
+            err[name] = rel_l2([r.velgrad[i] for r in grec], [r.velgrad[i] for r in rrec])
+    err["Es_shells"] = max(rel_l2(gsh[i, 0], rsh[i, 0]) for i in range(len(rsh)))
+    err["Ed_shells"] = max(rel_l2(gsh[i, 1], rsh[i, 1]) for i in range(len(rsh)))
+    for r in grec:
+        assert math.isfinite(r.Esspe)
+    return err
+
+
 def field(ia, ja, ka=0, k0=4.0, seed=0):
     return seeded_field(ia, ja, ka, k0=k0, seed=seed)

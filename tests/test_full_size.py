@@ -1,0 +1,77 @@
+"""Checks at the measured sizes (2048^2 and 256^3, the configurations the step throughput is
+quoted on), where running the CPU oracle for many steps would take hours:
+
+- one FP64 step at 2048^2 against the oracle (1e-12, every record value and spectrum shell);
+- the FP32 form against the FP64 form on the GPU after many steps (1e-5; the FP64 form is held
+  to the oracle at 1e-9 over 100 steps on smaller grids), the precision claim of the FP32 form;
+- run-to-run determinism: two runs from the same field give bit-identical records and state
+  (all reductions are fixed-order);
+- the 2/3 rule: the state read back has no energy outside the kept modes.
+"""
+import numpy as np
+import pytest
+
+from tests.parity_util import compare, compare_gpu_runs, field, make_params, run_gpu, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+# the step-throughput workloads: 2D band-forced with projection, 3D linearly forced
+W2D = dict(ia=2048, ja=2048, ka=0, reynolds=5000.0, deltat=1e-4, forcemethod=2, forcek=5, target_energy=0.075,
+           lprojectd=True, kmax=1 << 30)
+W3D = dict(ia=256, ja=256, ka=256, reynolds=5000.0, deltat=5e-4, forcemethod=1, forcek=5, target_energy=1.5,
+           lprojectd=False, kmax=85)
+
+
+def _params(w):
+    return make_params(**w)
+
+
+def _field(w):
+    return field(w["ia"], w["ja"], w["ka"], k0=4.0 if w["ka"] == 0 else 3.0, seed=0)
+
+
+def _check(err, tol, eta_tol=None):
+    bad = {k: v for k, v in err.items() if not (v <= (eta_tol if (k == "eta_min" and eta_tol) else tol))}
+    assert not bad, f"above {tol}: {bad}"
+
+
+def test_2d2048_fp64_one_step_matches_oracle(gpu_lib):
+    p, u = _params(W2D), _field(W2D)
+    _check(compare(run_oracle(p, u, 1), run_gpu(p, u, 1, "fp64")), 1e-12)
+
+
+@pytest.mark.parametrize("w,nsteps", [(W2D, 100), (W3D, 20)], ids=["2d2048_100", "3d256_20"])
+def test_fp32_form_against_fp64_form(gpu_lib, w, nsteps):
+    """The FP32 form's error against the FP64 form at the measured size.  eta_min is a pointwise
+    extremum of sqrt(nu/|div|), so FP32 round-off of one point enters it unsmoothed: 1e-4."""
+    p, u = _params(w), _field(w)
+    err = compare_gpu_runs(run_gpu(p, u, nsteps, "fp64"), run_gpu(p, u, nsteps, "fp32"))
+    _check(err, 1e-5, eta_tol=1e-4)
+
+
+@pytest.mark.parametrize("w,prec", [(W2D, "fp32"), (W3D, "fp32"), (W3D, "fp64")],
+                         ids=["2d2048_fp32", "3d256_fp32", "3d256_fp64"])
+def test_bitwise_reproducible(gpu_lib, w, prec):
+    p, u = _params(w), _field(w)
+    r1, s1, u1 = run_gpu(p, u, 5, prec)
+    r2, s2, u2 = run_gpu(p, u, 5, prec)
+    for a, b in zip(r1, r2):
+        va = np.array([a.Esspe, a.Edspe, a.k2Edspe, a.kMEdspe, a.factor, a.E, *a.velgrad])
+        vb = np.array([b.Esspe, b.Edspe, b.k2Edspe, b.kMEdspe, b.factor, b.E, *b.velgrad])
+        assert np.array_equal(va, vb, equal_nan=True)   # E is NaN for forcing that does not log it
+    assert np.array_equal(s1, s2)
+    assert all(np.array_equal(a, b) for a, b in zip(u1, u2))
+
+
+@pytest.mark.parametrize("w", [W2D, W3D], ids=["2d2048", "3d256"])
+def test_state_stays_dealiased(gpu_lib, w):
+    """After steps the returned field has no energy in modes the 2/3 rule removes."""
+    from oracle.bastr_oracle import dealias_mask, generate_wave
+    p, u = _params(w), _field(w)
+    _, _, uf = run_gpu(p, u, 3, "fp32")
+    ks = generate_wave(p)
+    m = dealias_mask(p, np.sqrt(sum(k * k for k in ks)))
+    for c in uf:
+        spec = np.fft.fftn(c)
+        out = np.abs(spec[~m])
+        assert out.max() <= 1e-9 * np.abs(spec).max()

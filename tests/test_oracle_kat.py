@@ -213,3 +213,84 @@ def test_random_phase_force_is_real_and_in_band():
             assert np.max(np.abs(f.imag)) < 1e-14 * max(1.0, np.max(np.abs(f.real)))
         assert np.all(phi[~band] == 0) and np.all(np.abs(phi[band]) <= np.pi)
         assert not np.array_equal(band_phases(p, 8, band), phi)   # a new draw every call
+
+
+def _hitgen_amplitude(p, bis):
+    """var2(|k|) of the generators (Bastrpp.F90:650-657 2D, 757-762 3D, 861-862 bis)."""
+    ks = generate_wave(p)
+    kk = np.sqrt(sum(k * k for k in ks))
+    kks = np.where(kk == 0, 1.0, kk)
+    fk = float(p.forcek)
+    var1 = kks ** 4 * np.exp(-2 * (kks / fk) ** 2)
+    if not bis:
+        var1 = np.where(kks >= fk, var1, fk ** 6 / kks ** 2 * math.exp(-2.0))
+    var2 = np.sqrt(var1 / (2 * np.pi * kks)) if p.ndims == 2 else np.sqrt(var1 / (4 * np.pi * kks ** 2))
+    return ks, kk, np.where(kk == 0, 0.0, var2)
+
+
+def _off_nyquist(p):
+    """Modes with no index at the Nyquist position: there the generators' wavenumber (+n/2 on
+    both partners) breaks the Hermitian pairing and the real part halves the mode."""
+    axes = [p.ia, p.ja] + ([p.ka] if p.ndims == 3 else [])
+    masks = [np.arange(n) != n // 2 for n in axes]
+    m = masks[0][None, :] & masks[1][:, None] if p.ndims == 2 else \
+        masks[0][None, None, :] & masks[1][None, :, None] & masks[2][:, None, None]
+    return m
+
+
+@pytest.mark.parametrize("dims", [(64, 64, 0), (32, 64, 0), (16, 16, 16)], ids=["2d", "2d_nonsquare", "3d"])
+def test_hitgen_spectrum_is_the_generators_and_energy_is_target(dims):
+    """The random phases do not touch the amplitudes: away from the Nyquist lines every mode of
+    the generated field has |u^|^2 = factor^2 var2(|k|)^2, whatever the random numbers; the
+    field is dilatational (u^ parallel to k) and mean |u|^2 = target_energy."""
+    from oracle.bastr_oracle import hitgen
+    p = Params(ia=dims[0], ja=dims[1], ka=dims[2], forcek=5, target_energy=0.075)
+    u, angle, st = hitgen(p, 0, seed=11)
+    n = p.npts
+    assert abs(sum(np.mean(c * c) for c in u) - 0.075) < 1e-15
+    us = [np.fft.fftn(c) / n for c in u]
+    ks, kk, var2 = _hitgen_amplitude(p, False)
+    m = _off_nyquist(p)
+    e = sum(np.abs(c) ** 2 for c in us)
+    want = (st["factor"] * var2) ** 2
+    assert np.max(np.abs(e - want)[m]) <= 1e-12 * want.max()
+    # curl-free: k_i u^_j - k_j u^_i = 0
+    for i in range(p.ndims):
+        for j in range(i + 1, p.ndims):
+            assert np.max(np.abs(ks[i] * us[j] - ks[j] * us[i])[m]) <= 1e-12 * np.sqrt(want.max()) * kk.max()
+    # random_angle is a phase in [-pi, pi] everywhere but k = 0, which keeps a uniform number
+    assert np.all(np.abs(angle) <= np.pi)
+    assert 0.0 < angle.flat[0] < 1.0
+
+
+def test_hitgen_bis_cancels_u2_theta():
+    """hitgen2dbis picks alpha so that <|u|^2 theta> = 0 for u = uA + alpha uB."""
+    from oracle.bastr_oracle import hitgen
+    p = Params(ia=64, ja=64, ka=0, forcek=5, target_energy=0.075)
+    u, _, st = hitgen(p, 1, seed=3)
+    n = p.npts
+    ks = generate_wave(p)
+    us = [np.fft.fftn(c) / n for c in u]
+    theta = (np.fft.ifftn(1j * (ks[0] * us[0] + ks[1] * us[1])) * n).real
+    w = (u[0] ** 2 + u[1] ** 2) * theta
+    assert abs(np.mean(w)) <= 1e-12 * np.mean(np.abs(w))
+    assert abs(st["residual"]) <= 1e-9 * max(abs(st[q]) for q in ("QX", "QY", "QZ", "QW")) * max(1.0, abs(st["alpha"])) ** 3
+    assert abs(sum(np.mean(c * c) for c in u) - 0.075) < 1e-15
+
+
+def test_hitgen_alpha_root_forms():
+    """Both branches of the reference's cubic formula give a root."""
+    from oracle.bastr_oracle import hitgen_alpha
+    for q in [(1.0, 2.0, 3.0, 4.0), (-6.0, 11.0, -6.0, 1.0), (0.3, -2.0, 0.1, 1.5)]:
+        a = hitgen_alpha(*q)
+        assert abs(q[0] + q[1] * a + q[2] * a * a + q[3] * a ** 3) < 1e-9
+
+
+def test_hitgen_uniform_stream():
+    """53-bit uniforms in (0, 1), distinct per draw and seed, reproducible."""
+    from oracle.bastr_oracle import hitgen_uniform
+    p = Params(ia=64, ja=64, ka=0)
+    a, b, c = hitgen_uniform(p, 0, 5), hitgen_uniform(p, 1, 5), hitgen_uniform(p, 0, 6)
+    assert np.array_equal(a, hitgen_uniform(p, 0, 5))
+    assert a.min() > 0.0 and a.max() < 1.0 and abs(a.mean() - 0.5) < 0.02
+    assert not np.array_equal(a, b) and not np.array_equal(a, c)
