@@ -283,7 +283,7 @@ cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const 
         if (e != cudaSuccess) return e;
         if (MODE == XM_RHS_VG) h->n_vg_blocks = grid;
         const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.K, phys = 2.0 * h->g.nx * h->g.ny * 8;
-        const double b = MODE == XM_RHS ? mix * 6 * cs : MODE == XM_RHS_VG ? mix * 9 * cs
+        const double b = MODE == XM_RHS ? mix * 6 * cs : MODE == XM_RHS_VG ? mix * 8 * cs
                        : MODE == XM_TO_PHYS ? mix * 2 * cs + phys : phys + mix * 2 * cs;
         ProfScope ps(h, MODE == XM_RHS_VG ? "k2d_xpass_vg" : MODE == XM_RHS ? "k2d_xpass" : "k2d_xpass_state", b);
         LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg, h->g,

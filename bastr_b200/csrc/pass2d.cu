@@ -90,11 +90,11 @@ template <typename T> __device__ __forceinline__ void st2(cplx<T>* dst, cplx<T> 
 // Pass A: inverse transforms along y of kx columns.
 // ---------------------------------------------------------------------------------------
 // Field sets: the state (u1, u2), the product's fields (g1, h1, g2, h2), the velocity-gradient
-// fields (q1, q2, t), or both of the last two from one read of the column (YI_RHS_VG).
+// fields (q1, q2 = ky^2 u^), or both of the last two from one read of the column (YI_RHS_VG).
 enum YInvSet : int { YI_STATE = 0, YI_RHS = 1, YI_VG = 2, YI_RHS_VG = 3 };
 
 template <typename T, typename TIN, int NY, int SET> struct YInv2D {
-    static constexpr int F = SET == YI_STATE ? 2 : SET == YI_RHS ? 4 : SET == YI_VG ? 3 : 7;   // fields produced
+    static constexpr int F = SET == YI_STATE ? 2 : SET == YI_RHS ? 4 : SET == YI_VG ? 2 : 6;   // fields produced
     static constexpr int F0 = SET == YI_VG ? 4 : 0;                                             // offset in MA
     static constexpr int UG = 2;                                             // units per sub-pass
     static constexpr int NG = (F + UG - 1) / UG;
@@ -142,7 +142,6 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
         const cplx<TIN>* col = stg + (size_t)gi * KY * 2;
         const int kx = item * G + gi;
         const bool valid = kx < K;
-        const T kxt = (T)kx;
         // the column's two components, in the register order of the first transform stage
         cplx<T> ra[EPT], rb[EPT];
 #pragma unroll
@@ -170,14 +169,11 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
                     f[2] = b; f[3] = cscale<T>(cmuli<T>(b), ky);
                 }
                 if constexpr (SET == YI_VG || SET == YI_RHS_VG) {
+                    // ky^2 u^: the x pass forms lap(u) = -(kx^2 u^ + this) per point
                     constexpr int o = SET == YI_VG ? 0 : 4;
                     const T ky2 = ky * ky;
                     f[o + 0] = cscale<T>(a, ky2);
                     f[o + 1] = cscale<T>(b, ky2);
-                    // lap(theta)^ = -i |k|^2 (kx u1^ + ky u2^)   (solution.F90:1131)
-                    const T kk = kxt * kxt + ky2;
-                    f[o + 2] = cscale<T>(cmulni<T>(cadd<T>(cscale<T>(a, kxt), cscale<T>(b, ky))), kk);
-                    f[o + 3] = mk<T>(0, 0);
                 }
 #pragma unroll
                 for (int u = 0; u < UG; ++u) v[u * EPT + e] = f[grp * UG + u];
@@ -205,8 +201,10 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
 enum XMode : int { XM_RHS = 1, XM_RHS_VG = 2, XM_TO_PHYS = 3, XM_FROM_PHYS = 4 };
 
 template <typename T, int NX, int MODE> struct XPass2D {
-    static constexpr int ZU = MODE == XM_RHS ? 3 : MODE == XM_RHS_VG ? 5 : 1;   // units per row
+    static constexpr int ZU = MODE == XM_RHS ? 3 : MODE == XM_RHS_VG ? 4 : 1;   // units per row
+    // fields in the staged records (records of 4), and how many of them are read
     static constexpr int FIN = MODE == XM_RHS ? 4 : MODE == XM_RHS_VG ? 8 : MODE == XM_TO_PHYS ? 2 : 0;
+    static constexpr int FLIVE = MODE == XM_RHS_VG ? 6 : FIN;
     static constexpr int EPT = ept_fit<NX, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_XPASS_F32>();
     // at most three units share one shared-memory exchange; more run as a second transform
     static constexpr int ZA = ZU > 3 ? 3 : ZU, ZB = ZU - ZA;
@@ -272,8 +270,9 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
             for (int i = threadIdx.x; i < total; i += NT) {
                 const int q = i / C16, c = i - q * C16;
                 const int kp = q / G, r = q - kp * G;
-                if (r < nrow) {
-                    const int k = kp / NPIN, pr = kp - k * NPIN;
+                const int k = kp / NPIN, pr = kp - k * NPIN;
+                // chunks holding only fields past FLIVE are never read
+                if (r < nrow && pr * W + c * (16 / (int)sizeof(cplx<T>)) < P::FLIVE) {
                     cp_async16(stg + (size_t)i * 16,
                                MA + (((size_t)k * (ftot / W) + pr) * NY + y0 + r) * W + c * (16 / (int)sizeof(cplx<T>)));
                 }
@@ -324,11 +323,10 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                         v[EPT + e] = pack_at<T>(cscale<T>(cmuli<T>(g1), kx), cscale<T>(cmuli<T>(g2), kx), hi, z0);
                         v[2 * EPT + e] = pack_at<T>(h1, h2, hi, z0);
                         if constexpr (MODE == XM_RHS_VG) {
-                            const cplx<T> q1 = src(4), q2 = src(5), th = src(6);
+                            const cplx<T> q1 = src(4), q2 = src(5);
                             const T kx2 = kx * kx;
                             v[3 * EPT + e] = pack_at<T>(csub<T>(cscale<T>(g1, -kx2), q1),
                                                         csub<T>(cscale<T>(g2, -kx2), q2), hi, z0);
-                            v[4 * EPT + e] = pack_at<T>(th, mk<T>(0, 0), hi, z0);
                         }
                     }
                 }
@@ -367,15 +365,21 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                         if (valid) {
                             // velgrad_calculate2D (solution.F90:1149-1166): per-point terms in the
                             // compute precision, sums in FP64; eta_min = sqrt(nu/max|theta|) is
-                            // formed once from the largest |theta| (the map is monotone)
-                            const cplx<T> l = v[3 * EPT + e], th = v[4 * EPT + e];
+                            // formed once from the largest |theta| (the map is monotone).
+                            // dissp = <2 u_i theta lap(u_i) + |u|^2 lap(theta)>, with the second
+                            // mean taken as <theta lap(|u|^2)> = <theta (2 u_i lap(u_i) +
+                            // 2 |grad u_i|^2)>: equal on the grid (every product has degree
+                            // 3(K-1) < n per axis, so grid means are exact and integration by
+                            // parts holds), and it needs no lap(theta) field
+                            const cplx<T> l = v[3 * EPT + e];
                             const T nuT = (T)nu;
                             const T div = u1x + u2y;
                             const T uu = u1 * u1 + u2 * u2;
+                            const T gg = u1x * u1x + u1y * u1y + u2x * u2x + u2y * u2y;
                             acc[0] += (double)(div * div * uu);
                             acc[1] += (double)((u1x * u1x + u2y * u2y + (T)2 * u1y * u2x) * uu);
                             acc[2] += (double)(div * uu);
-                            acc[3] += (double)((T)2 * u1 * div * l.x + (T)2 * u2 * div * l.y + uu * th.x);
+                            acc[3] += (double)(div * ((T)4 * (u1 * l.x + u2 * l.y) + (T)2 * gg));
                             acc[4] += (double)(nuT * (u1y - u2x) * (u1y - u2x) + nuT * div * div);
                             divmax = fmax(divmax, (double)fabs(div));
                             acc[5] += (double)uu;
