@@ -601,12 +601,23 @@ cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_forcing(bastr_handle* h, double* rec) {
+// The forcing of a step, and the velocity-gradient statistics of the step (when vg) in the same
+// single-block kernel; without forcing they get their own launch.
+cudaError_t launch_forcing(bastr_handle* h, double* rec, bool vg) {
     const int m = h->p.forcemethod;
-    if (m == 0) return cudaSuccess;
+    const double* vgp = vg ? h->vg_part : nullptr;
+    const int vgn = vg ? h->n_vg_blocks : 0;
+    if (m == 0) {
+        if (vg) {
+            ProfScope ps(h, "k_velgrad_final", (double)h->n_vg_blocks * 64);
+            LAUNCH(launch_k(h, k_velgrad_final<256>, 1, 256, 0, h->vg_part, h->n_vg_blocks, h->g, rec));
+        }
+        return cudaGetLastError();
+    }
     if (m == 1) {
         ProfScope ps(h, "k_force_linear", (double)h->n_en_blocks * 8);
-        LAUNCH(launch_k(h, k_force_linear<256>, 1, 256, 0, h->en_part, h->n_en_blocks, rec, h->p.target_energy, h->pend));
+        LAUNCH(launch_k(h, k_force_linear<256>, 1, 256, 0, h->en_part, h->n_en_blocks, rec, h->p.target_energy, h->pend,
+                        vgp, vgn, h->g));
         h->scale_pending = true;
         return cudaGetLastError();
     }
@@ -619,10 +630,10 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec) {
         ProfScope ps(h, "k_force_band", 0);
         if (h->g.d == 2)
             LAUNCH(launch_k(h, k_force_band<2, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
-                            h->rng));
+                            h->rng, vgp, vgn));
         else
             LAUNCH(launch_k(h, k_force_band<3, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
-                            h->rng));
+                            h->rng, vgp, vgn));
     }
     return cudaGetLastError();
 }
@@ -634,12 +645,9 @@ cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
     cudaError_t e = launch_spectra(h, rec, sh);
     if (e != cudaSuccess) return e;
     if (h->p.timemethod == 1) {
+        // the statistics' partials (first stage) stay untouched until the forcing kernel sums them
         e = launch_rhs(h, EPI_RK1, true, vg);
         if (e != cudaSuccess) return e;
-        if (vg) {
-            ProfScope ps(h, "k_velgrad_final", (double)h->n_vg_blocks * 64);
-            LAUNCH(launch_k(h, k_velgrad_final<256>, 1, 256, 0, h->vg_part, h->n_vg_blocks, h->g, rec));
-        }
         e = launch_rhs(h, EPI_RK2, false, false);
         if (e != cudaSuccess) return e;
         e = launch_rhs(h, EPI_RK3, false, false);
@@ -648,13 +656,9 @@ cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
         for (int s = 1; s <= 6; ++s) {
             e = launch_rhs(h, s == 6 ? EPI_CN_LAST : EPI_CN_MID, s == 1, vg && s == 1);
             if (e != cudaSuccess) return e;
-            if (vg && s == 1) {
-                ProfScope ps(h, "k_velgrad_final", (double)h->n_vg_blocks * 64);
-                LAUNCH(launch_k(h, k_velgrad_final<256>, 1, 256, 0, h->vg_part, h->n_vg_blocks, h->g, rec));
-            }
         }
     }
-    return launch_forcing(h, rec);
+    return launch_forcing(h, rec, vg);
 }
 
 int count_launches(bastr_handle* h, bool vg) {
@@ -664,8 +668,9 @@ int count_launches(bastr_handle* h, bool vg) {
     n += per_rhs * nrhs;
     if (h->g.d == 2 && BASTR_FUSE_Y) n -= nrhs - 1;  // pass A of every stage but the first is fused
     if (h->g.d == 2 && vg) n -= 1;                   // 2D: one pass A makes the product and statistics fields
-    if (vg) n += 2;                                 // extra inverse pass + final reduction
     const int m = h->p.forcemethod;
+    if (vg) n += m == 0 ? 2 : 1;                    // extra inverse pass; the final reduction runs in
+                                                    // the forcing kernel, or alone without forcing
     if (m == 1) n += 1;
     else if (m == 2) n += 1;
     else if (m == 3 || m == 4) n += 2;

@@ -273,11 +273,18 @@ __global__ void __launch_bounds__(NT) k_sum_partials(const double* __restrict__ 
 // fixed order to sum_k w|u^|^2 = mean(|u|^2) (Parseval with the 1/N forward normalisation);
 // factor = sqrt(target / mean(|u|^2/2)).  The scale u *= factor itself is left pending: the
 // next step's spectra kernel (or k_apply_pending) applies it.
+// With vg_nblk > 0 the kernel first finishes the step's velocity-gradient statistics from the x
+// pass's partials (they are read only from the record, so they need no launch of their own).
 template <int NT>
 __global__ void __launch_bounds__(NT) k_force_linear(const double* __restrict__ part, int n,
-                                                     double* __restrict__ rec, double target, double2* pend) {
+                                                     double* __restrict__ rec, double target, double2* pend,
+                                                     const double* __restrict__ vg_part, int vg_nblk, Geo g) {
     pdl_wait();
-    __shared__ double scratch[NT];
+    __shared__ double scratch[7 * NT];
+    if (vg_nblk > 0) {
+        velgrad_finish<NT>(vg_part, vg_nblk, g, rec, scratch);
+        __syncthreads();
+    }
     double acc[1] = {0};
     for (int b = threadIdx.x; b < n; b += NT) acc[0] += part[b];
     block_sum<1, NT>(acc, scratch);
@@ -338,9 +345,14 @@ __device__ __forceinline__ double band_phase(int kx, int ky, int kz, unsigned lo
 template <int D, int NT>
 __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo g, int method, int forcek,
                                                    double target, int project2d, double* __restrict__ rec,
-                                                   unsigned long long* rng) {
+                                                   unsigned long long* rng, const double* __restrict__ vg_part,
+                                                   int vg_nblk) {
     pdl_wait();
-    __shared__ double scratch[2 * NT];
+    __shared__ double scratch[7 * NT];
+    if (vg_nblk > 0) {   // the step's velocity-gradient statistics, as k_force_linear does
+        velgrad_finish<NT>(vg_part, vg_nblk, g, rec, scratch);
+        __syncthreads();
+    }
     const bool rnd = method == 3 || method == 4;
     const unsigned long long ctr = rnd ? *rng : 0ull;
     const int s = forcek;

@@ -164,3 +164,19 @@ def test_random_phase_forcing_matches_oracle(gpu_lib, dims, method):
     for n, tol in ((1, 1e-12), (10, 1e-9)):
         err = compare(run_oracle(p, u, n), run_gpu(p, u, n, "fp64"))
         _check(err, tol)
+
+
+@pytest.mark.parametrize("dims,kw", [
+    ((64, 64, 0), dict(forcemethod=2, lprojectd=True)), ((64, 64, 0), dict(forcemethod=0)),
+    ((64, 64, 0), dict(forcemethod=1, timemethod=2)), ((32, 32, 32), dict(forcemethod=1)),
+    ((32, 32, 32), dict(forcemethod=3)), ((32, 32, 32), dict(forcemethod=0))],
+    ids=["2d_band", "2d_none", "2d_linear_cn", "3d_linear", "3d_random", "3d_none"])
+def test_launch_count_matches_profiled_launches(gpu_lib, dims, kw):
+    """The launches per step the library reports (the bench's gpu_launches) are the kernels a
+    step actually launches, counted by the per-launch profiler."""
+    from bastr_b200 import BastrGPU
+    ia, ja, ka = dims
+    with BastrGPU(ia, ja, ka, target_energy=1.0, **kw) as s:
+        s.set_state(field(ia, ja, ka, k0=3.0, seed=1))
+        stats = s.profile(3)
+        assert sum(k["launches"] for k in stats) == 3 * s.info()["launches_per_step"]
