@@ -220,9 +220,16 @@ template <typename T, int NX, int MODE> struct XPass2D {
     static constexpr int NT = G * NTR;
     static constexpr int MINB = G > G0 ? 1 : (BASTR_MINB_XPASS > 0 && sizeof(T) == 4 && MODE == XM_RHS) ? BASTR_MINB_XPASS : minb_for<T, NT>();
     static constexpr int KMAX = NX / 3;
-    // one staged group: G rows of K*FIN mixed values, or G rows of 2 physical components
+    // one staged group: G rows of K*FIN mixed values, or G rows of 2 physical components.  The
+    // threads of a warp read consecutive wavenumbers, so the staged run of one wavenumber is an
+    // odd number of 16-byte units long (padded if need be): a multiple of 32 bytes would put the
+    // threads' addresses a multiple of the bank width apart (4- to 8-way conflicts).  With one
+    // row per block the dead tail of the last record (fields past FLIVE) is not staged.
+    static constexpr int KBASE = (FLIVE < FIN && G == 1) ? FLIVE : FIN * G;
+    static constexpr int KPAD = (KBASE * (int)sizeof(cplx<T>) / 16) % 2 == 0 ? 16 / (int)sizeof(cplx<T>) : 0;
+    static constexpr int KSTR = KBASE + KPAD;                                // elements per kx
     static constexpr size_t STAGE = MODE == XM_FROM_PHYS ? (size_t)G * 2 * NX * sizeof(double)
-                                                          : (size_t)G * KMAX * FIN * sizeof(cplx<T>);
+                                                          : (size_t)KMAX * KSTR * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
     static constexpr size_t TWB = BASTR_XPASS_TW_SMEM ? tw_smem_bytes<T, NX>() : 0;
@@ -263,7 +270,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
             stage_line(d, phys_in + (size_t)y0 * NX, nrow * NX * 8);
             stage_line(d + G * NX, phys_in + (size_t)NY * NX + (size_t)y0 * NX, nrow * NX * 8);
         } else {
-            // rows y0.. of every (kx, pair) -> staging [kx][pair][row][2]
+            // rows y0.. of every (kx, pair) -> staging [kx][pair][row][W], KSTR elements per kx
             constexpr int W = FIN < 4 ? FIN : 4;
             constexpr int NPIN = FIN / W, C16 = W * (int)sizeof(cplx<T>) / 16;
             const int total = K * NPIN * G * C16;
@@ -273,7 +280,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 const int k = kp / NPIN, pr = kp - k * NPIN;
                 // chunks holding only fields past FLIVE are never read
                 if (r < nrow && pr * W + c * (16 / (int)sizeof(cplx<T>)) < P::FLIVE) {
-                    cp_async16(stg + (size_t)i * 16,
+                    cp_async16(stg + (size_t)k * P::KSTR * sizeof(cplx<T>) + (size_t)((pr * G + r) * C16 + c) * 16,
                                MA + (((size_t)k * (ftot / W) + pr) * NY + y0 + r) * W + c * (16 / (int)sizeof(cplx<T>)));
                 }
             }
@@ -310,7 +317,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 // K = floor(NX/3) in 2D: these elements are dealiased zeros for every thread
                 if (IFFT::in_band(e, NX / 3 + 1)) continue;
                 if (valid && (lo || hi)) {
-                    const cplx<T>* src0 = row + (size_t)k * (FIN / W) * G * W;
+                    const cplx<T>* src0 = row + (size_t)k * P::KSTR;
                     auto src = [&](int f) { return src0[(f / W) * G * W + (f % W)]; };
                     const bool z0 = p == 0;
                     const cplx<T> g1 = src(0);

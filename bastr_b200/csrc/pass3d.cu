@@ -268,9 +268,17 @@ template <typename T, int NX, int MODE> struct XPass3D {
     static constexpr int G = groups_per_block<NTR>() > 16 ? 16 : groups_per_block<NTR>();
     static constexpr int NT = G * NTR;
     static constexpr int KMAX = NX / 3;
+    // staging [kx][f][row]: the threads of a warp touch consecutive wavenumbers, so one
+    // wavenumber's run is made an odd number of 16-byte units long (a multiple of 32 bytes puts
+    // the threads a multiple of the bank width apart), and in FP32 a tile row of one wavenumber
+    // an odd number of elements (4-way conflicts otherwise; FP64 has 2-way ones and keeps its
+    // tile unpadded, which leaves the velocity-gradient variant two blocks per SM)
+    static constexpr int KPAD = (FIN * G * (int)sizeof(cplx<T>) / 16) % 2 == 0 ? 16 / (int)sizeof(cplx<T>) : 0;
+    static constexpr int KSTR = FIN * G + KPAD;        // staged elements per kx
+    static constexpr int TSTR = sizeof(T) == 4 ? ((3 * G) | 1) : 3 * G;   // tile elements per kx
     static constexpr size_t STAGE = MODE == X3_FROM_PHYS ? (size_t)G * 3 * NX * sizeof(double)
-                                                          : (size_t)G * KMAX * FIN * sizeof(cplx<T>);
-    static constexpr size_t TILE = (size_t)KMAX * G * 3 * sizeof(cplx<T>);   // output tile [kx][row][c]
+                                                          : (size_t)KMAX * KSTR * sizeof(cplx<T>);
+    static constexpr size_t TILE = (size_t)KMAX * TSTR * sizeof(cplx<T>);   // output tile [kx][row][c]
     static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
     static constexpr size_t SMEM = STAGE + TILE + XCHR;
@@ -311,9 +319,11 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
             const char* src = reinterpret_cast<const char*>(MB + (size_t)z0 * K * FIN * NY + y0);
             for (int i = threadIdx.x; i < total; i += NT) {
                 const int kf = i / NCH, c = i - kf * NCH;
+                const int k = kf / FIN;
                 const char* sp = src + ((size_t)kf * NY * sizeof(cplx<T>)) + c * CH;
-                if constexpr (CH == 16) cp_async16(d + (size_t)kf * RB + c * CH, sp);
-                else cp_async8(d + (size_t)kf * RB + c * CH, sp);
+                char* dp = d + (size_t)k * P::KSTR * sizeof(cplx<T>) + (size_t)(kf - k * FIN) * RB + c * CH;
+                if constexpr (CH == 16) cp_async16(dp, sp);
+                else cp_async8(dp, sp);
             }
         }
         cp_async_commit();
@@ -349,7 +359,7 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
                 // K = floor(NX/3): these elements are dealiased zeros for every thread
                 if (IFFT::in_band(e, NX / 3 + 1)) continue;
                 if (valid && (lo || hi)) {
-                    const cplx<T>* src0 = rw + (size_t)k * FIN * G;
+                    const cplx<T>* src0 = rw + (size_t)k * P::KSTR;
                     auto src = [&](int f) { return src0[f * G]; };
                     const bool z0 = p == 0;
                     if constexpr (MODE == X3_TO_PHYS) {
@@ -445,7 +455,7 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
             __syncthreads();
             for (int k = t; k < K; k += NTR) {
                 const int km = k == 0 ? 0 : NX - k;
-                cplx<T>* dst = tile + ((size_t)k * G + gi) * 3;
+                cplx<T>* dst = tile + (size_t)k * P::TSTR + gi * 3;
                 const cplx<T> Z = sm[pidx(k)], Zc = cconj<T>(sm[pidx(km)]);
                 const cplx<T> W = sm[US + pidx(k)], Wc = cconj<T>(sm[US + pidx(km)]);
                 dst[0] = cscale<T>(cadd<T>(Z, Zc), (T)0.5);
@@ -457,7 +467,7 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
             const int r0 = item * G, z0 = r0 / NY, y0 = r0 - z0 * NY;
             for (int i = threadIdx.x; i < K * G * 3; i += NT) {
                 const int k = i / (G * 3), rem = i - k * (G * 3);
-                MC[(((size_t)z0 * K + k) * NY + y0) * 3 + rem] = tile[i];
+                MC[(((size_t)z0 * K + k) * NY + y0) * 3 + rem] = tile[(size_t)k * P::TSTR + rem];
             }
         }
     }
