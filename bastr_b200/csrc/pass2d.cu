@@ -108,7 +108,7 @@ template <typename T, typename TIN, int NY, int SET> struct YInv2D {
     __host__ __device__ static size_t stage_bytes(int KY) {
         return ((size_t)G * KY * 2 * sizeof(cplx<TIN>) + 15) & ~(size_t)15;
     }
-    static constexpr size_t TWB = tw_smem_bytes<T, NY>();
+    static constexpr size_t TWB = tw_stage_bytes<T, FFT>();
     static size_t smem(int KY) { return stage_bytes(KY) + XCH + TWB; }
 };
 
@@ -124,7 +124,12 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
     const int K = g.K, KY = g.KY;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY)) + gi * FFT::SMEM_ELEMS;
-    tw = stage_twiddles<T, NY>(reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY) + P::XCH), tw);
+    constexpr bool STW = P::TWB > 0;   // twiddles by stage in shared memory
+    if constexpr (STW) {
+        cplx<T>* d = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY) + P::XCH);
+        FFT::fill_stage_twiddles(d, tw);
+        tw = d;
+    }
     pdl_wait();
     const int nitems = (K + G - 1) / G;
     const int colbytes = KY * 2 * (int)sizeof(cplx<TIN>);
@@ -178,7 +183,7 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
 #pragma unroll
                 for (int u = 0; u < UG; ++u) v[u * EPT + e] = f[grp * UG + u];
             }
-            FFT::run(v, sm, tw, t);
+            FFT::template run<STW>(v, sm, tw, t);
             if (valid) {
                 // record width W = min(4, ftot) fields: MA[kx][group][y][W]
                 const int W = ftot < 4 ? ftot : 4;
@@ -232,7 +237,7 @@ template <typename T, int NX, int MODE> struct XPass2D {
                                                           : (size_t)KMAX * KSTR * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
-    static constexpr size_t TWB = BASTR_XPASS_TW_SMEM ? tw_smem_bytes<T, NX>() : 0;
+    static constexpr size_t TWB = BASTR_XPASS_TW_SMEM ? tw_stage_bytes<T, IFFT, FFFT>() : 0;
     static constexpr size_t SMEM = STAGE + XCHR + TWB;
 };
 
@@ -258,7 +263,18 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
     unsigned char* stg = smraw;
     const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * IFFT::SMEM_ELEMS;
-    if constexpr (P::TWB > 0) tw = stage_twiddles<T, NX>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
+    // twiddles by stage in shared memory: the inverse plan (shared by IFFT and IFFTB), then the forward one
+    constexpr bool STW = P::TWB > 0;
+    static_assert(P::IFFTB::TWS_ELEMS == IFFT::TWS_ELEMS, "one inverse plan");
+    const cplx<T>* twi = tw;
+    const cplx<T>* twf = tw;
+    if constexpr (STW) {
+        cplx<T>* d = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR);
+        IFFT::fill_stage_twiddles(d, tw);
+        FFFT::fill_stage_twiddles(d + IFFT::TWS_ELEMS, tw);
+        twi = d;
+        twf = d + IFFT::TWS_ELEMS;
+    }
     pdl_wait();
     const int K = g.K, NY = g.ny;
     const int nitems = (NY + G - 1) / G;
@@ -342,8 +358,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
         __syncthreads();   // the staging buffer is free: fetch the next row group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
         if constexpr (MODE != XM_FROM_PHYS) {
-            IFFT::run(v, sm, tw, t);
-            if constexpr (P::ZB > 0) P::IFFTB::run(v + P::ZA * EPT, sm, tw, t);
+            IFFT::template run<STW>(v, sm, twi, t);
+            if constexpr (P::ZB > 0) P::IFFTB::template run<STW>(v + P::ZA * EPT, sm, twi, t);
         }
 
         if constexpr (MODE == XM_TO_PHYS) {
@@ -396,7 +412,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 }
             }
             // forward transform of the packed product (or of the packed physical fields)
-            FFFT::run(v, sm, tw, t);
+            FFFT::template run<STW>(v, sm, twf, t);
             // split the packed spectrum into the two half spectra, kx in [0,K): Z[k] and Z[NX-k]
 #pragma unroll
             for (int e = 0; e < EPT; ++e) {
@@ -441,7 +457,7 @@ template <typename T, int NY> struct YFwd2D {
     static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
-    static constexpr size_t TWB = tw_smem_bytes<T, NY>();
+    static constexpr size_t TWB = tw_stage_bytes<T, FFT>();
     static constexpr size_t SMEM = STAGE + XCHR + TWB;
 };
 
@@ -456,7 +472,12 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
     cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
-    tw = stage_twiddles<T, NY>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
+    constexpr bool STW = P::TWB > 0;   // twiddles by stage in shared memory
+    if constexpr (STW) {
+        cplx<T>* d = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR);
+        FFT::fill_stage_twiddles(d, tw);
+        tw = d;
+    }
     pdl_wait();
     const int K = g.K, KY = g.KY;
     const int nitems = (K + G - 1) / G;
@@ -495,7 +516,7 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
         }
         __syncthreads();   // the staging buffer is free: fetch the next column group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
-        FFT::run(v, sm, tw, t);
+        FFT::template run<STW>(v, sm, tw, t);
         if (valid) {
             const double w = kx == 0 ? 1.0 : 2.0;
             const bool from_u0 = input_is_u0 != 0;
@@ -564,7 +585,7 @@ template <typename T, int NY> struct YFwdInv2D {
     static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
-    static constexpr size_t TWB = tw_smem_bytes<T, NY>();
+    static constexpr size_t TWB = tw_stage_bytes<T, FFT, IFFT>();
     static constexpr size_t SMEM = STAGE + XCHR + TWB;
 };
 
@@ -582,7 +603,17 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
     cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * FFT::SMEM_ELEMS;
-    tw = stage_twiddles<T, NY>(reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR), tw);
+    // twiddles by stage in shared memory: the forward plan, then the inverse one
+    constexpr bool STW = P::TWB > 0;
+    const cplx<T>* twf = tw;
+    const cplx<T>* twi = tw;
+    if constexpr (STW) {
+        cplx<T>* d = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR);
+        FFT::fill_stage_twiddles(d, tw);
+        IFFT::fill_stage_twiddles(d + FFT::TWS_ELEMS, tw);
+        twf = d;
+        twi = d + FFT::TWS_ELEMS;
+    }
     pdl_wait();
     const int K = g.K, KY = g.KY;
     const int nitems = (K + G - 1) / G;
@@ -621,7 +652,7 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
         }
         __syncthreads();   // the staging buffer is free: fetch the next column group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
-        FFT::run(v, sm, tw, t);
+        FFT::template run<STW>(v, sm, twf, t);
         // the next stage input at the positions this thread holds (zero outside the kept set)
         cplx<T> nx[2 * EPT];
 #pragma unroll
@@ -674,7 +705,7 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
                 u[e] = nx[c * EPT + e];
                 u[EPT + e] = cscale<T>(cmuli<T>(nx[c * EPT + e]), ky);
             }
-            IFFT::run(u, sm, tw, t);
+            IFFT::template run<STW>(u, sm, twi, t);
             if (valid) {
                 cplx<T>* dst = MA + (size_t)kx * (FTOT / W) * NY * W + 2 * c;
 #pragma unroll

@@ -69,7 +69,32 @@ struct RegFFT {
         return b >= lo && b + NTR - 1 <= N - lo;
     }
 
-    template <int R, int PS>
+    // Twiddles by stage, an alternative layout of the same values: for every stage s >= 1 the
+    // base powers w^(j k S), j = 1, 2, 4, 8 (as many as the stage's radix uses), k = 0..PS-1,
+    // j-major.  The threads of a warp take consecutive k, so they read consecutive elements;
+    // in the linear table w^m they read with stride j*S, a multiple of the bank width for most
+    // stages.  Same values, same arithmetic: results are bitwise those of the linear table.
+    static constexpr int nbase(int R) { return R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4; }
+    static constexpr int tws_off(int s) {
+        return s <= 1 ? 0 : tws_off(s - 1) + PL::sub(INV, s - 1) * nbase(PL::radix(INV, s - 1));
+    }
+    static constexpr int TWS_ELEMS = NS > 1 ? tws_off(NS) : 0;
+
+    // Block-wide copy of the linear table `lin` (w^m, m < N/2) into the by-stage layout at dst
+    // (TWS_ELEMS elements); the caller's next __syncthreads() publishes it.
+    template <int S = 1>
+    __device__ static __forceinline__ void fill_stage_twiddles(cplx<T>* dst, const cplx<T>* __restrict__ lin) {
+        if constexpr (S < NS) {
+            constexpr int R = PL::radix(INV, S), PS = PL::sub(INV, S), NB = nbase(R), TS = N / (PS * R);
+            for (int i = threadIdx.x; i < NB * PS; i += blockDim.x) {
+                const int jb = i / PS, k = i - jb * PS;
+                dst[tws_off(S) + i] = lin[(1 << jb) * k * TS];
+            }
+            fill_stage_twiddles<S + 1>(dst, lin);
+        }
+    }
+
+    template <int R, int PS, int S_, bool STAGED>
     __device__ static __forceinline__ void compute(cplx<T>* v, const cplx<T>* __restrict__ tw, int t) {
 #pragma unroll
         for (int q = 0; q < EPT / R; ++q) {
@@ -77,20 +102,25 @@ struct RegFFT {
             if constexpr (PS > 1) {
                 constexpr int S = N / (PS * R);
                 const int k = b & (PS - 1);
+                // w[j] = w^(j k S): read for j = 1, 2, 4, 8, products for the rest
+                auto base = [&](int jb) -> cplx<T> {
+                    if constexpr (STAGED) return tw[tws_off(S_) + jb * PS + k];
+                    else return tw[(1 << jb) * k * S];
+                };
                 cplx<T> w[R];
-                w[1] = tw[k * S];
+                w[1] = base(0);
                 if constexpr (R >= 4) {
-                    w[2] = tw[2 * k * S];
+                    w[2] = base(1);
                     w[3] = cmul<T>(w[2], w[1]);
                 }
                 if constexpr (R >= 8) {
-                    w[4] = tw[4 * k * S];
+                    w[4] = base(2);
                     w[5] = cmul<T>(w[4], w[1]);
                     w[6] = cmul<T>(w[4], w[2]);
                     w[7] = cmul<T>(w[4], w[3]);
                 }
                 if constexpr (R >= 16) {
-                    w[8] = tw[8 * k * S];
+                    w[8] = base(3);
 #pragma unroll
                     for (int j = 9; j < 16; ++j) w[j] = cmul<T>(w[8], w[j - 8]);
                 }
@@ -132,45 +162,38 @@ struct RegFFT {
         __syncthreads();
     }
 
-    template <int S>
+    template <int S, bool STAGED>
     __device__ static __forceinline__ void stages(cplx<T>* v, cplx<T>* sm, const cplx<T>* __restrict__ tw, int t) {
         if constexpr (S < NS) {
             constexpr int R = PL::radix(INV, S);
             constexpr int PS = PL::sub(INV, S);
-            compute<R, PS>(v, tw, t);
+            compute<R, PS, S, STAGED>(v, tw, t);
             if constexpr (S + 1 < NS) {
                 exchange<R, PS, PL::radix(INV, S + 1)>(v, sm, t);
             }
-            stages<S + 1>(v, sm, tw, t);
+            stages<S + 1, STAGED>(v, sm, tw, t);
         }
     }
 
-    // v: UPT*EPT registers (unit-major); sm: this group's SMEM_ELEMS shared elements.
+    // v: UPT*EPT registers (unit-major); sm: this group's SMEM_ELEMS shared elements; tw: the
+    // linear table w^m, or with STAGED the by-stage table of fill_stage_twiddles.
     // The caller fills v in in_pos order; on return v holds the transform in out_pos order.
     // Contains __syncthreads(): every thread of the block must call it.
+    template <bool STAGED = false>
     __device__ static __forceinline__ void run(cplx<T>* v, cplx<T>* sm, const cplx<T>* __restrict__ tw, int t) {
-        stages<0>(v, sm, tw, t);
+        stages<0, STAGED>(v, sm, tw, t);
     }
 };
 
 // Twiddles a length-N RegFFT reads: w^m for m < N/2 (the largest index any stage forms is
-// R/2 * k * N/(PS*R) < N/2).  Kernels copy them into shared memory once per block.
+// R/2 * k * N/(PS*R) < N/2).  With BASTR_TW_SMEM the kernels keep them in shared memory in the
+// by-stage layout (fill_stage_twiddles); otherwise the transforms read the linear table.
 #ifndef BASTR_TW_SMEM
 #define BASTR_TW_SMEM 1
 #endif
-template <typename T, int N> constexpr size_t tw_smem_bytes() {
-    return BASTR_TW_SMEM ? (size_t)(N / 2) * sizeof(cplx<T>) : 0;
-}
-// Copies the table into `dst` (tw_smem_bytes<T, N>() of shared memory) and returns the table
-// the transforms should read; the caller's next __syncthreads() publishes the copy.
-template <typename T, int N>
-__device__ __forceinline__ const cplx<T>* stage_twiddles(cplx<T>* dst, const cplx<T>* __restrict__ src) {
-    if constexpr (BASTR_TW_SMEM) {
-        for (int i = threadIdx.x; i < N / 2; i += blockDim.x) dst[i] = src[i];
-        return dst;
-    } else {
-        return src;
-    }
+// Shared bytes of the by-stage tables of the transforms F... (one after the other).
+template <typename T, class... F> constexpr size_t tw_stage_bytes() {
+    return BASTR_TW_SMEM ? (size_t)(0 + ... + F::TWS_ELEMS) * sizeof(cplx<T>) : 0;
 }
 
 }  // namespace bastr
