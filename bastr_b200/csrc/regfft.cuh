@@ -137,7 +137,7 @@ struct RegFFT {
     }
 
     // Shared-memory position of element a of a unit during the exchanges.  The padded map pidx
-    // leaves the warps of the radix-8 FP32 plans and the radix-4 FP64 plans with 1.2-1.3x the
+    // leaves the warps of the radix-8 FP32 plans and the radix-4 and -8 FP64 plans with 1.2-1.3x the
     // ideal number of shared-memory wavefronts (bank conflicts of the stride-PS writes); for
     // those plans an XOR of the low bank bits with higher bits spreads every exchange over all
     // banks.  Each swizzle changes bit i only by bits above i, so it is a bijection within every
@@ -146,6 +146,7 @@ struct RegFFT {
     __device__ static __forceinline__ int sidx(int a) {
         if constexpr (sizeof(T) == 4 && EPT == 8 && N <= 512) return a ^ (((a >> 3) ^ (a >> 5)) & 15);
         else if constexpr (sizeof(T) == 8 && EPT == 4) return a ^ (((a >> 2) ^ (a >> 5)) & 7);
+        else if constexpr (sizeof(T) == 8 && EPT == 8) return a ^ (((a >> 3) ^ (a >> 4)) & 7);
         else return pidx(a);
     }
 
