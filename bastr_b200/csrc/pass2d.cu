@@ -86,6 +86,19 @@ template <typename T> __device__ __forceinline__ void st2(cplx<T>* dst, cplx<T> 
     }
 }
 
+// Two adjacent complex values (16-byte aligned in FP32) as one vector load: half the load
+// instructions, and a warp's 16-byte loads of consecutive pairs fill every bank once.
+template <typename T> __device__ __forceinline__ void ld2(const cplx<T>* src, cplx<T>& a, cplx<T>& b) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(src);
+        a = make_float2(q.x, q.y);
+        b = make_float2(q.z, q.w);
+    } else {
+        a = src[0];
+        b = src[1];
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // Pass A: inverse transforms along y of kx columns.
 // ---------------------------------------------------------------------------------------
@@ -333,20 +346,24 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 // K = floor(NX/3) in 2D: these elements are dealiased zeros for every thread
                 if (IFFT::in_band(e, NX / 3 + 1)) continue;
                 if (valid && (lo || hi)) {
+                    // field f of this wavenumber at src0[(f / W) * G * W + f % W]: pairs (0,1), (2,3),
+                    // (4,5) are adjacent and 16-byte aligned
                     const cplx<T>* src0 = row + (size_t)k * P::KSTR;
-                    auto src = [&](int f) { return src0[(f / W) * G * W + (f % W)]; };
                     const bool z0 = p == 0;
-                    const cplx<T> g1 = src(0);
+                    cplx<T> g1, h1;
+                    ld2<T>(src0, g1, h1);
                     if constexpr (MODE == XM_TO_PHYS) {
-                        v[e] = pack_at<T>(g1, src(1), hi, z0);
+                        v[e] = pack_at<T>(g1, h1, hi, z0);
                     } else {
-                        const cplx<T> h1 = src(1), g2 = src(2), h2 = src(3);
+                        cplx<T> g2, h2;
+                        ld2<T>(src0 + 2, g2, h2);
                         const T kx = (T)k;
                         v[e] = pack_at<T>(g1, g2, hi, z0);
                         v[EPT + e] = pack_at<T>(cscale<T>(cmuli<T>(g1), kx), cscale<T>(cmuli<T>(g2), kx), hi, z0);
                         v[2 * EPT + e] = pack_at<T>(h1, h2, hi, z0);
                         if constexpr (MODE == XM_RHS_VG) {
-                            const cplx<T> q1 = src(4), q2 = src(5);
+                            cplx<T> q1, q2;
+                            ld2<T>(src0 + G * W, q1, q2);
                             const T kx2 = kx * kx;
                             v[3 * EPT + e] = pack_at<T>(csub<T>(cscale<T>(g1, -kx2), q1),
                                                         csub<T>(cscale<T>(g2, -kx2), q2), hi, z0);
@@ -511,8 +528,8 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
 #pragma unroll
         for (int e = 0; e < EPT; ++e) {
             const int y = FFT::in_pos(t, e);
-            v[e] = valid ? col[2 * y] : mk<T>(0, 0);
-            v[EPT + e] = valid ? col[2 * y + 1] : mk<T>(0, 0);
+            if (valid) ld2<T>(col + 2 * y, v[e], v[EPT + e]);
+            else v[e] = v[EPT + e] = mk<T>(0, 0);
         }
         __syncthreads();   // the staging buffer is free: fetch the next column group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
@@ -647,8 +664,8 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
 #pragma unroll
         for (int e = 0; e < EPT; ++e) {
             const int y = FFT::in_pos(t, e);
-            v[e] = valid ? col[2 * y] : mk<T>(0, 0);
-            v[EPT + e] = valid ? col[2 * y + 1] : mk<T>(0, 0);
+            if (valid) ld2<T>(col + 2 * y, v[e], v[EPT + e]);
+            else v[e] = v[EPT + e] = mk<T>(0, 0);
         }
         __syncthreads();   // the staging buffer is free: fetch the next column group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
