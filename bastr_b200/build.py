@@ -1,46 +1,103 @@
 """Builds the in-tree CUDA library ``bastr_b200/libbastr_gpu.so`` for sm_100a.
 
 Run ``python -m bastr_b200.build`` (or ``__graft_entry__.build()``).  nvcc cross-compiles,
-so no GPU is needed.  The library is rebuilt only when a source is newer than it.
+so no GPU is needed.  The library is split into translation units (the C ABI, the 2D and 3D
+step schedules per compute precision, the allocation-free spectra) that compile in parallel
+into ``bastr_b200/_build/``; an object is rebuilt only when one of its sources is newer than it,
+and the library is relinked when an object is newer than it.
 """
 from __future__ import annotations
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
+OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libbastr_gpu.so")
-SOURCES = ["capi.cu", "noalloc.cu"]
-DEPS = ["capi.cu", "pass2d.cu", "pass3d.cu", "diag.cu", "ensemble.cu", "fullfft.cu", "closure.cu", "transfer.cu", "hitgen.cu", "noalloc.cu", "fft_engine.cuh", "regfft.cuh",
-        "solver.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+HEADER = os.path.join(ROOT, "include", "bastr_gpu.h")
+
+_COMMON = ["handle.cuh", "solver.cuh", "fft_engine.cuh", "regfft.cuh"]
+# translation unit -> the sources it includes
+UNITS = {
+    "capi.cu": _COMMON + ["diag.cu", "fullfft.cu", "closure.cu", "transfer.cu", "hitgen.cu", "ensemble.cu"],
+    "steps2d_f32.cu": _COMMON + ["pass2d.cu", "steps2d.cuh"],
+    "steps2d_f64.cu": _COMMON + ["pass2d.cu", "steps2d.cuh"],
+    "steps3d_f32.cu": _COMMON + ["pass2d.cu", "pass3d.cu", "steps3d.cuh"],
+    "steps3d_f64.cu": _COMMON + ["pass2d.cu", "pass3d.cu", "steps3d.cuh"],
+    "noalloc.cu": ["solver.cuh", "fft_engine.cuh"],
+}
+# every source file of the library (for callers that check staleness as a whole)
+DEPS = sorted({d for u, ds in UNITS.items() for d in ds + [u]})
+FLAGS = ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+         "--expt-relaxed-constexpr"]
+
+
+def _obj(unit: str) -> str:
+    return os.path.join(OBJDIR, unit[:-3] + ".o")
+
+
+def _mtime(p: str) -> float:
+    return os.path.getmtime(p) if os.path.exists(p) else float("inf")
+
+
+def _unit_stale(unit: str) -> bool:
+    o = _obj(unit)
+    if not os.path.exists(o):
+        return True
+    t = os.path.getmtime(o)
+    srcs = [os.path.join(CSRC, d) for d in UNITS[unit] + [unit]] + [HEADER]
+    return any(_mtime(s) > t for s in srcs)
 
 
 def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, d) for d in DEPS] + [os.path.join(ROOT, "include", "bastr_gpu.h")]
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    return any(_unit_stale(u) or os.path.getmtime(_obj(u)) > t for u in UNITS)
 
 
-def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None, jobs: int | None = None) -> str:
+    """Compiles the stale translation units in parallel and links the library.  `extra` flags
+    (e.g. -D overrides) apply to every unit and force a full rebuild."""
+    if extra:
+        force = True
     if not force and not _stale():
         return LIB
-    cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
-           "-I", os.path.join(ROOT, "include"),
-           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES], *(extra or [])]
+    os.makedirs(OBJDIR, exist_ok=True)
+    todo = [u for u in UNITS if force or _unit_stale(u)]
+
+    def compile_unit(unit):
+        cmd = [NVCC, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, unit),
+               "-o", _obj(unit) + ".tmp", *(extra or [])]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode == 0:
+            os.replace(_obj(unit) + ".tmp", _obj(unit))
+        return unit, r
+
+    njobs = jobs or min(len(todo), max(1, os.cpu_count() or 1)) or 1
+    failed = []
+    with ThreadPoolExecutor(max_workers=njobs) as ex:
+        for unit, r in ex.map(compile_unit, todo):
+            if r.returncode != 0:
+                failed.append(unit)
+                sys.stderr.write(r.stdout + r.stderr)
+    if failed:
+        raise RuntimeError(f"nvcc failed for {', '.join(failed)}")
+    link = [NVCC, *ARCH, "--shared", "-Xcompiler", "-fPIC", "-o", LIB + ".tmp", *[_obj(u) for u in UNITS]]
     if verbose:
-        print(" ".join(cmd), flush=True)
-    r = subprocess.run(cmd, capture_output=True, text=True)
+        print(" ".join(link), flush=True)
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed for libbastr_gpu.so")
+        raise RuntimeError("link of libbastr_gpu.so failed")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,539 +1,16 @@
-// C ABI of the B200 Burgers time step: handle, device buffers, launch schedule.
-//
-// One translation unit: the pass kernels are included so that every template instance the
-// schedule needs is generated here.
-#include <cuda_runtime.h>
-
-#include <algorithm>
-#include <cmath>
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
-#include <map>
-#include <mutex>
-#include <set>
-#include <tuple>
-#include <string>
-#include <vector>
-
-#include "../../include/bastr_gpu.h"
-#ifndef BASTR_PDL
-#define BASTR_PDL 1
-#endif
-// Returns the launch error from the enclosing cudaError_t function.
-#define LAUNCH(...)                                 \
-    do {                                            \
-        cudaError_t le_ = (__VA_ARGS__);            \
-        if (le_ != cudaSuccess) return le_;         \
-    } while (0)
+// C ABI of the B200 Burgers time step: handle creation, the step loop with its diagnostics and
+// forcing, state transfer, records, profiling, and the post-processing entry points.  The pass
+// schedules of the right-hand side live in steps2d_*.cu / steps3d_*.cu.
+#include "handle.cuh"
 #include "diag.cu"
-#include "pass2d.cu"
-#include "pass3d.cu"
 #include "fullfft.cu"
 #include "closure.cu"
 #include "transfer.cu"
 #include "hitgen.cu"
 
-using namespace bastr;
+using namespace bastr_impl;
 
 namespace {
-
-constexpr int kChunk = 256;   // records kept on the device per batch chunk
-
-struct Twiddles {
-    int n = 0;
-    double2* d64 = nullptr;
-    float2* d32 = nullptr;
-};
-
-}  // namespace
-
-struct bastr_handle {
-    bastr_params p{};
-    Geo g{};
-    int fp32 = 0;
-    int allkmax = 0;
-    int nshell = 0;            // shells 0..K cover every kept mode
-    int64_t nstep = 0;
-    double time = 0.0;
-    bool have_state = false;
-    std::string err;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    // device buffers
-    double2* u0 = nullptr;     // truncated state, FP64
-    void* us = nullptr;        // stage input (compute precision)
-    void* acc = nullptr;       // RK accumulator (compute precision)
-    void* ma = nullptr;        // mixed fields after the first inverse pass(es)
-    void* mb = nullptr;        // mixed fields before the last forward pass(es)
-    void* mc = nullptr;        // 3D only: second mixed buffer
-    double* phys = nullptr;    // physical fields for set/get (d * npts)
-    double* vg_part = nullptr;
-    double* en_part = nullptr;
-    unsigned int* done = nullptr;  // completion tickets of last-block reductions [kTickets]
-    int share_log2 = 0;            // plan: persistent grids use 1/2^share_log2 of the resident blocks
-    bool ma_ready = false;         // 2D: MA already holds pass A of the next stage
-    float* closure_buf = nullptr;  // 3D closure: tau_hat [3][n] (allocated on first use)
-    double2* tr_buf = nullptr;     // transfer spectra: full complex grids (allocated on first use)
-    double* tr_modes = nullptr;    // transfer spectra: per-mode values, item partials, shell sums
-    double* hg_part = nullptr;     // initial-field generators: per-block partial sums
-    double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
-    unsigned long long* rng = nullptr;  // forcing calls so far: counter of the random-phase stream
-    bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
-    double* shell = nullptr;   // [nshell][4]
-    double* rec = nullptr;     // [kChunk][R_COUNT]
-    double* shells_dev = nullptr; // [kChunk][2][allkmax+1]
-    int64_t dev_bytes = 0;
-    size_t n_state = 0;        // complex entries of the truncated state (all components)
-    int n_vg_blocks = 0;
-    int n_en_blocks = 0;
-    int launches_per_step = 0;
-    int chunk_used = 0;        // records written by the last async batch
-    int64_t batch_n0 = 0;      // nstep and time at the start of that batch
-    double batch_t0 = 0.0;
-    Twiddles tw[3];            // per axis x, y, z
-    size_t n_disk = 0;         // kept modes with |k| < K (state entries the spectra kernel reads, per component)
-    // shell mode lists for the spectra (CSR): modes grouped by shell, cut into work items
-    int* sp_modes = nullptr;
-    int* sp_item_lo = nullptr;   // [n_items + 1]
-    int* sp_shell_item = nullptr; // [nshell + 1]
-    double* sp_item_part = nullptr;
-    int n_items = 0;
-    // per-launch profiling (bastr_profile): CUDA events around every launch
-    bool prof_on = false;
-    std::vector<cudaEvent_t> ev_pool;
-    size_t ev_used = 0;
-    struct ProfRec { const char* name; size_t ev; double bytes; };
-    std::vector<ProfRec> prof;
-    std::vector<double> kn;
-    std::vector<int64_t> ecount;
-};
-
-namespace {
-
-// Slots of h->done: one per kind of last-block reduction (each stays 0 between launches).
-enum Ticket : int { T_SPECTRA = 0, kTickets = 4 };
-
-int fail(bastr_handle* h, int code, const char* fmt, ...) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    if (h) h->err = buf;
-    return code;
-}
-
-#define CK(call)                                                                          \
-    do {                                                                                  \
-        cudaError_t e_ = (call);                                                          \
-        if (e_ != cudaSuccess)                                                            \
-            return fail(h, BASTR_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
-                        __FILE__, __LINE__);                                              \
-    } while (0)
-
-bool is_pow2(int n) { return n >= 16 && n <= 2048 && (n & (n - 1)) == 0; }
-
-// Brackets one kernel launch with CUDA events when profiling is on; `bytes` is the launch's
-// algorithmic traffic (unique global reads plus writes of its inputs and outputs).
-struct ProfScope {
-    bastr_handle* h;
-    size_t ev = 0;
-    bool on = false;
-    ProfScope(bastr_handle* hh, const char* name, double bytes) : h(hh) {
-        if (!h->prof_on || h->ev_used + 2 > h->ev_pool.size()) return;
-        ev = h->ev_used;
-        h->ev_used += 2;
-        on = true;
-        cudaEventRecord(h->ev_pool[ev], h->stream);
-        h->prof.push_back({name, ev, bytes});
-    }
-    ~ProfScope() {
-        if (on) cudaEventRecord(h->ev_pool[ev + 1], h->stream);
-    }
-};
-
-// Global traffic of the state-side reads/writes of one epilogue over n entries.
-double epi_bytes(int epi, bool from_u0, double n, double cs) {
-    switch (epi) {
-        case EPI_STORE: return n * 16;
-        case EPI_RK1: return n * 16 + 2 * n * cs;
-        case EPI_RK2: return 2 * n * cs + n * 16 + 2 * n * cs;
-        case EPI_RK3: return 2 * n * cs + n * 16 + n * 16;
-        case EPI_CN_MID: return from_u0 ? n * 16 + n * cs : 2 * n * cs + n * 16;
-        case EPI_CN_LAST: return n * cs + 2 * n * 16;
-    }
-    return 0;
-}
-
-template <typename T> const cplx<T>* twp(const Twiddles& t);
-template <> const cplx<double>* twp<double>(const Twiddles& t) { return t.d64; }
-template <> const cplx<float>* twp<float>(const Twiddles& t) { return t.d32; }
-
-// Launches a kernel of the step on the handle's stream with programmatic dependent launch: it may
-// start while the previous kernel drains, and waits for it on the device (pdl_wait).
-template <typename... KArgs, typename... Args>
-cudaError_t launch_k(bastr_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
-                     Args&&... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = h->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = BASTR_PDL;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
-
-// Enables the dynamic shared memory a kernel instance asks for and returns how many of its
-// blocks fit on one SM; both once per (device, kernel).
-std::mutex g_prep_mu;
-std::map<std::tuple<int, const void*, size_t>, int> g_prepped;
-int g_num_sms[64] = {};
-template <typename K> cudaError_t prep(K kernel, size_t smem, int nt = 0, int* blocks_per_sm = nullptr) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    const auto key = std::make_tuple(dev, (const void*)kernel, smem);
-    std::lock_guard<std::mutex> lk(g_prep_mu);
-    auto it = g_prepped.find(key);
-    if (it == g_prepped.end()) {
-        if (smem > 48 * 1024) {
-            e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        int nb = 1;
-        if (nt > 0) {
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, nt, smem);
-            if (e != cudaSuccess) return e;
-            if (nb < 1) nb = 1;
-        }
-        if (dev >= 0 && dev < 64 && g_num_sms[dev] == 0) {
-            e = cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev);
-            if (e != cudaSuccess) return e;
-        }
-        it = g_prepped.emplace(key, nb).first;
-    }
-    if (blocks_per_sm) *blocks_per_sm = it->second;
-    return cudaSuccess;
-}
-
-// Grid of a persistent pass: as many blocks as fit on the device, at most one per work item.
-// The handle's plan may restrict its persistent grids to 1/2^share of that (an ensemble runs
-// many handles at once, each on a share of the SMs).
-template <typename K> cudaError_t persistent_grid(const bastr_handle* h, K kernel, size_t smem, int nt, int nitems,
-                                                  int* grid) {
-    int nb = 1;
-    cudaError_t e = prep(kernel, smem, nt, &nb);
-    if (e != cudaSuccess) return e;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const int sms = (dev >= 0 && dev < 64 && g_num_sms[dev] > 0) ? g_num_sms[dev] : 148;
-    *grid = std::max(1, std::min(nitems, (nb * sms) >> h->share_log2));
-    return cudaSuccess;
-}
-
-#define SIZE_CASES(N, ...)                      \
-    switch (N) {                                 \
-        case 16: { constexpr int NN = 16; __VA_ARGS__; } break;     \
-        case 32: { constexpr int NN = 32; __VA_ARGS__; } break;     \
-        case 64: { constexpr int NN = 64; __VA_ARGS__; } break;     \
-        case 128: { constexpr int NN = 128; __VA_ARGS__; } break;   \
-        case 256: { constexpr int NN = 256; __VA_ARGS__; } break;   \
-        case 512: { constexpr int NN = 512; __VA_ARGS__; } break;   \
-        case 1024: { constexpr int NN = 1024; __VA_ARGS__; } break; \
-        case 2048: { constexpr int NN = 2048; __VA_ARGS__; } break; \
-        default: return cudaErrorInvalidValue;   \
-    }
-
-int cdiv(int a, int b) { return (a + b - 1) / b; }
-
-// ---------------------------------------------------------------------------------------
-// 2D launches
-// ---------------------------------------------------------------------------------------
-template <typename T, typename TIN, int SET>
-cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
-    SIZE_CASES(h->g.ny, {
-        using P = YInv2D<T, TIN, NN, SET>;
-        auto k = k2d_yinv<T, TIN, NN, SET>;
-        const size_t smem = P::smem(h->g.KY);
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, smem, P::NT, cdiv(h->g.K, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        const double K_ = h->g.K;
-        ProfScope ps(h, SET == YI_VG ? "k2d_yinv_vg" : SET == YI_RHS_VG ? "k2d_yinv_rhs_vg" : "k2d_yinv",
-                     K_ * h->g.KY * 2 * sizeof(cplx<TIN>) + (double)h->g.ny * K_ * P::F * sizeof(cplx<T>));
-        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[1])));
-    });
-    return cudaGetLastError();
-}
-
-template <typename T, int MODE>
-cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const double* pin, double* pout,
-                     double* vg) {
-    SIZE_CASES(h->g.nx, {
-        using P = XPass2D<T, NN, MODE>;
-        auto k = k2d_xpass<T, NN, MODE>;
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.ny, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        if (MODE == XM_RHS_VG) h->n_vg_blocks = grid;
-        const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.K, phys = 2.0 * h->g.nx * h->g.ny * 8;
-        const double b = MODE == XM_RHS ? mix * 6 * cs : MODE == XM_RHS_VG ? mix * 8 * cs
-                       : MODE == XM_TO_PHYS ? mix * 2 * cs + phys : phys + mix * 2 * cs;
-        ProfScope ps(h, MODE == XM_RHS_VG ? "k2d_xpass_vg" : MODE == XM_RHS ? "k2d_xpass" : "k2d_xpass_state", b);
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg, h->g,
-                                                twp<T>(h->tw[0])));
-    });
-    return cudaGetLastError();
-}
-
-template <typename T, int EPI>
-cudaError_t l2_yfwd(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0) {
-    SIZE_CASES(h->g.ny, {
-        using P = YFwd2D<T, NN>;
-        auto k = k2d_yfwd<T, NN, EPI>;
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        if (io.energy_part) h->n_en_blocks = grid;
-        const double cs = sizeof(cplx<T>);
-        ProfScope ps(h, "k2d_yfwd", (double)h->g.K * h->g.ny * 2 * cs +
-                                    epi_bytes(EPI, from_u0, (double)h->g.K * h->g.KY * 2, cs));
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1])));
-    });
-    return cudaGetLastError();
-}
-
-template <typename T, int EPI>
-cudaError_t l2_yfwd_inv(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0, void* MA) {
-    SIZE_CASES(h->g.ny, {
-        using P = YFwdInv2D<T, NN>;
-        auto k = k2d_yfwd_inv<T, NN, EPI>;
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        const double cs = sizeof(cplx<T>);
-        ProfScope ps(h, "k2d_yfwd_inv", (double)h->g.K * h->g.ny * 2 * cs +
-                                        epi_bytes(EPI, from_u0, (double)h->g.K * h->g.KY * 2, cs) +
-                                        (double)h->g.ny * h->g.K * 4 * cs);
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]),
-                        (cplx<T>*)MA));
-    });
-    return cudaGetLastError();
-}
-
-#ifndef BASTR_FUSE_Y
-#define BASTR_FUSE_Y 1
-#endif
-
-// One right-hand-side evaluation F(u_s) and its combination, 2D.  Stages after the first find
-// their pass A already done when the previous stage's forward pass handed its stage input on
-// (k2d_yfwd_inv, h->ma_ready).
-template <typename T>
-cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
-    cudaError_t e = cudaSuccess;
-    const int ftot = vg ? 8 : 4;
-    if (from_u0 && vg) e = l2_yinv<T, double, YI_RHS_VG>(h, h->u0, h->ma, ftot);
-    else if (from_u0) e = l2_yinv<T, double, YI_RHS>(h, h->u0, h->ma, ftot);
-    else if (!h->ma_ready || vg) e = l2_yinv<T, T, YI_RHS>(h, h->us, h->ma, ftot);
-    h->ma_ready = false;
-    if (e != cudaSuccess) return e;
-    if (vg) {
-        if (!from_u0) {   // the statistics are of the state u0
-            e = l2_yinv<T, double, YI_VG>(h, h->u0, h->ma, ftot);
-            if (e != cudaSuccess) return e;
-        }
-        e = l2_xpass<T, XM_RHS_VG>(h, h->ma, ftot, h->mb, nullptr, nullptr, h->vg_part);
-    } else {
-        e = l2_xpass<T, XM_RHS>(h, h->ma, ftot, h->mb, nullptr, nullptr, nullptr);
-    }
-    if (e != cudaSuccess) return e;
-    StageIO<T> io{h->u0, (cplx<T>*)h->us, (cplx<T>*)h->acc, nullptr};
-    const bool need_en = (epi == EPI_RK3 || epi == EPI_CN_LAST) &&
-                         (h->p.forcemethod == 1 || h->p.forcemethod >= 3);
-    if (need_en) io.energy_part = h->en_part;
-    if (BASTR_FUSE_Y && (epi == EPI_RK1 || epi == EPI_RK2 || epi == EPI_CN_MID)) {
-        h->ma_ready = true;
-        switch (epi) {
-            case EPI_RK1: return l2_yfwd_inv<T, EPI_RK1>(h, h->mb, io, from_u0, h->ma);
-            case EPI_RK2: return l2_yfwd_inv<T, EPI_RK2>(h, h->mb, io, from_u0, h->ma);
-            case EPI_CN_MID: return l2_yfwd_inv<T, EPI_CN_MID>(h, h->mb, io, from_u0, h->ma);
-        }
-    }
-    switch (epi) {
-        case EPI_RK1: return l2_yfwd<T, EPI_RK1>(h, h->mb, io, from_u0);
-        case EPI_RK2: return l2_yfwd<T, EPI_RK2>(h, h->mb, io, from_u0);
-        case EPI_RK3: return l2_yfwd<T, EPI_RK3>(h, h->mb, io, from_u0);
-        case EPI_CN_MID: return l2_yfwd<T, EPI_CN_MID>(h, h->mb, io, from_u0);
-        case EPI_CN_LAST: return l2_yfwd<T, EPI_CN_LAST>(h, h->mb, io, from_u0);
-    }
-    return cudaErrorInvalidValue;
-}
-
-// ---------------------------------------------------------------------------------------
-// 3D launches
-// ---------------------------------------------------------------------------------------
-#define SIZE_CASES3(N, ...)                                  \
-    switch (N) {                                              \
-        case 16: { constexpr int NN = 16; __VA_ARGS__; } break;     \
-        case 32: { constexpr int NN = 32; __VA_ARGS__; } break;     \
-        case 64: { constexpr int NN = 64; __VA_ARGS__; } break;     \
-        case 128: { constexpr int NN = 128; __VA_ARGS__; } break;   \
-        case 256: { constexpr int NN = 256; __VA_ARGS__; } break;   \
-        case 512: { constexpr int NN = 512; __VA_ARGS__; } break;   \
-        default: return cudaErrorInvalidValue;                \
-    }
-
-template <typename T, typename TIN, int SET>
-cudaError_t l3_zinv(bastr_handle* h, const void* S, void* MA, int ftot) {
-    SIZE_CASES3(h->g.nz, {
-        using P = ZInv3D<T, TIN, NN, SET>;
-        auto k = k3d_zinv<T, TIN, NN, SET>;
-        const size_t smem = P::smem(h->g.KZ);
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, smem, P::NT, cdiv(h->g.K * h->g.KY, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        const double lines = (double)h->g.K * h->g.KY;
-        ProfScope ps(h, SET == ZI_VG ? "k3d_zinv_vg" : "k3d_zinv",
-                     lines * h->g.KZ * 3 * sizeof(cplx<TIN>) + lines * h->g.nz * P::F * sizeof(cplx<T>));
-        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<TIN>*)S, (cplx<T>*)MA, ftot, h->g, twp<T>(h->tw[2])));
-    });
-    return cudaGetLastError();
-}
-
-template <typename T, int SET>
-cudaError_t l3_yinv(bastr_handle* h, const void* MA, void* MB) {
-    SIZE_CASES3(h->g.ny, {
-        using P = YInv3D<T, NN, SET>;
-        auto k = k3d_yinv<T, NN, SET>;
-        const size_t smem = P::smem(h->g.KY);
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, smem, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        const double cs = sizeof(cplx<T>);
-        ProfScope ps(h, SET == YB_RHS_VG ? "k3d_yinv_vg" : "k3d_yinv",
-                     (double)h->g.K * h->g.nz * (h->g.KY * P::FIN + h->g.ny * P::F) * cs);
-        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<T>*)MA, (cplx<T>*)MB, h->g, twp<T>(h->tw[1])));
-    });
-    return cudaGetLastError();
-}
-
-template <typename T, int MODE>
-cudaError_t l3_xpass(bastr_handle* h, const void* MB, void* MC, const double* pin, double* pout, double* vg) {
-    SIZE_CASES3(h->g.nx, {
-        using P = XPass3D<T, NN, MODE>;
-        auto k = k3d_xpass<T, NN, MODE>;
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.ny * h->g.nz, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        if (MODE == X3_RHS_VG) h->n_vg_blocks = grid;
-        const double cs = sizeof(cplx<T>), mix = (double)h->g.ny * h->g.nz * h->g.K;
-        const double phys = 3.0 * h->g.nx * h->g.ny * h->g.nz * 8;
-        const double b = MODE == X3_RHS ? mix * 12 * cs : MODE == X3_RHS_VG ? mix * 16 * cs
-                       : MODE == X3_TO_PHYS ? mix * 3 * cs + phys : phys + mix * 3 * cs;
-        ProfScope ps(h, MODE == X3_RHS_VG ? "k3d_xpass_vg" : MODE == X3_RHS ? "k3d_xpass" : "k3d_xpass_state", b);
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg, h->g,
-                                                twp<T>(h->tw[0])));
-    });
-    return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t l3_yfwd(bastr_handle* h, const void* MC, void* MD) {
-    SIZE_CASES3(h->g.ny, {
-        using P = YFwd3D<T, NN>;
-        auto k = k3d_yfwd<T, NN>;
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        ProfScope ps(h, "k3d_yfwd", (double)h->g.K * h->g.nz * (h->g.ny + h->g.KY) * 3 * sizeof(cplx<T>));
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MC, (cplx<T>*)MD, h->g, twp<T>(h->tw[1])));
-    });
-    return cudaGetLastError();
-}
-
-template <typename T, int EPI>
-cudaError_t l3_zfwd(bastr_handle* h, const void* MD, StageIO<T> io, int from_u0) {
-    SIZE_CASES3(h->g.nz, {
-        using P = ZFwd3D<T, NN>;
-        auto k = k3d_zfwd<T, NN, EPI>;
-        int grid = 1;
-        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K * h->g.KY, P::G), &grid);
-        if (e != cudaSuccess) return e;
-        if (io.energy_part) h->n_en_blocks = grid;
-        const double cs = sizeof(cplx<T>), lines = (double)h->g.K * h->g.KY;
-        ProfScope ps(h, "k3d_zfwd", lines * h->g.nz * 3 * cs + epi_bytes(EPI, from_u0, lines * h->g.KZ * 3, cs));
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MD, io, from_u0, h->g, twp<T>(h->tw[2])));
-    });
-    return cudaGetLastError();
-}
-
-// Mixed-field buffer sizes (bytes) for compute element size cs.
-void sizes3d(bastr_handle* h, size_t cs, size_t& ma, size_t& mb, size_t& mc) {
-    const Geo& g = h->g;
-    const size_t K = g.K, KY = g.KY, NY = g.ny, NZ = g.nz;
-    const size_t c64 = sizeof(double2);
-    ma = std::max({K * NZ * KY * 10 * cs, K * KY * NZ * 3 * cs, K * NZ * KY * 3 * c64, K * KY * NZ * 3 * c64});
-    mb = std::max(NZ * NY * K * 13 * cs, NZ * NY * K * 3 * c64);
-    mc = std::max(NZ * K * NY * 3 * cs, NZ * K * NY * 3 * c64);
-}
-
-template <typename T>
-cudaError_t rhs3d(bastr_handle* h, int epi, bool from_u0, bool vg) {
-    cudaError_t e;
-    const int ftot = vg ? 10 : 6;
-    if (from_u0) e = l3_zinv<T, double, ZI_RHS>(h, h->u0, h->ma, ftot);
-    else e = l3_zinv<T, T, ZI_RHS>(h, h->us, h->ma, ftot);
-    if (e != cudaSuccess) return e;
-    if (vg) {
-        e = l3_zinv<T, double, ZI_VG>(h, h->u0, h->ma, ftot);
-        if (e != cudaSuccess) return e;
-        e = l3_yinv<T, YB_RHS_VG>(h, h->ma, h->mb);
-        if (e != cudaSuccess) return e;
-        e = l3_xpass<T, X3_RHS_VG>(h, h->mb, h->mc, nullptr, nullptr, h->vg_part);
-    } else {
-        e = l3_yinv<T, YB_RHS>(h, h->ma, h->mb);
-        if (e != cudaSuccess) return e;
-        e = l3_xpass<T, X3_RHS>(h, h->mb, h->mc, nullptr, nullptr, nullptr);
-    }
-    if (e != cudaSuccess) return e;
-    e = l3_yfwd<T>(h, h->mc, h->ma);
-    if (e != cudaSuccess) return e;
-    StageIO<T> io{h->u0, (cplx<T>*)h->us, (cplx<T>*)h->acc, nullptr};
-    const bool need_en = (epi == EPI_RK3 || epi == EPI_CN_LAST) &&
-                         (h->p.forcemethod == 1 || h->p.forcemethod >= 3);
-    if (need_en) io.energy_part = h->en_part;
-    switch (epi) {
-        case EPI_RK1: return l3_zfwd<T, EPI_RK1>(h, h->ma, io, from_u0);
-        case EPI_RK2: return l3_zfwd<T, EPI_RK2>(h, h->ma, io, from_u0);
-        case EPI_RK3: return l3_zfwd<T, EPI_RK3>(h, h->ma, io, from_u0);
-        case EPI_CN_MID: return l3_zfwd<T, EPI_CN_MID>(h, h->ma, io, from_u0);
-        case EPI_CN_LAST: return l3_zfwd<T, EPI_CN_LAST>(h, h->ma, io, from_u0);
-    }
-    return cudaErrorInvalidValue;
-}
-
-cudaError_t state3d_to_spectral(bastr_handle* h) {
-    cudaError_t e = l3_xpass<double, X3_FROM_PHYS>(h, nullptr, h->mc, h->phys, nullptr, nullptr);
-    if (e != cudaSuccess) return e;
-    e = l3_yfwd<double>(h, h->mc, h->ma);
-    if (e != cudaSuccess) return e;
-    StageIO<double> io{h->u0, nullptr, nullptr, nullptr};
-    return l3_zfwd<double, EPI_STORE>(h, h->ma, io, 0);
-}
-
-cudaError_t state3d_to_physical(bastr_handle* h) {
-    cudaError_t e = l3_zinv<double, double, ZI_STATE>(h, h->u0, h->ma, 3);
-    if (e != cudaSuccess) return e;
-    e = l3_yinv<double, YB_STATE>(h, h->ma, h->mb);
-    if (e != cudaSuccess) return e;
-    return l3_xpass<double, X3_TO_PHYS>(h, h->mb, nullptr, nullptr, h->phys, nullptr);
-}
 
 // One axis of the full-grid transform on the device array A (complex, [nz][ny][nx]).
 template <bool INV> cudaError_t full_axis(bastr_handle* h, double2* A, int axis, double scale) {
@@ -581,21 +58,24 @@ cudaError_t launch_rhs(bastr_handle* h, int epi, bool from_u0, bool vg) {
     return h->fp32 ? rhs3d<float>(h, epi, from_u0, vg) : rhs3d<double>(h, epi, from_u0, vg);
 }
 
-cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out) {
+// halt_code: the value the spectra kernel stores in the handle's stop word when Es+Ed is NaN
+// (the step's record slot + 1), 0 outside a batch of steps.
+cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out, unsigned int halt_code) {
     if (h->n_items > 0) {
         ProfScope ps(h, "k_spectra", (double)h->n_disk * (h->g.d * 16 + 4));
         if (h->g.d == 2)
             LAUNCH(launch_k(h, k_spectra_fused<2, 256>, h->n_items, 256, 0, h->u0, h->g, h->pend, h->sp_modes,
                             h->sp_item_lo, h->sp_item_part, h->done + T_SPECTRA, h->sp_shell_item, h->nshell,
-                            h->allkmax, rec, shells_out));
+                            h->allkmax, rec, shells_out, halt_code));
         else
             LAUNCH(launch_k(h, k_spectra_fused<3, 256>, h->n_items, 256, 0, h->u0, h->g, h->pend, h->sp_modes,
                             h->sp_item_lo, h->sp_item_part, h->done + T_SPECTRA, h->sp_shell_item, h->nshell,
-                            h->allkmax, rec, shells_out));
+                            h->allkmax, rec, shells_out, halt_code));
     } else {
         ProfScope ps(h, "k_spectra_final", 0);
         LAUNCH(launch_k(h, k_spectra_items_final<256>, 1, 256, 0, h->sp_item_part, h->sp_shell_item, h->nshell,
-                                                              h->allkmax, rec, shells_out, h->pend));
+                                                              h->allkmax, rec, shells_out, h->pend, h->g,
+                                                              halt_code));
     }
     h->scale_pending = false;
     return cudaGetLastError();
@@ -623,7 +103,7 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec, bool vg) {
     }
     if (m >= 3) {
         ProfScope ps(h, "k_sum_partials", (double)h->n_en_blocks * 8);
-        LAUNCH(launch_k(h, k_sum_partials<256>, 1, 256, 0, h->en_part, h->n_en_blocks, 1.0, rec, R_ENERGY));
+        LAUNCH(launch_k(h, k_sum_partials<256>, 1, 256, 0, h->en_part, h->n_en_blocks, 1.0, rec, R_ENERGY, h->g));
     }
     {
         const int proj = (m == 5 && h->g.d == 2 && h->p.lprojectd) ? 1 : 0;
@@ -642,7 +122,7 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec, bool vg) {
 cudaError_t launch_step(bastr_handle* h, int slot, bool vg) {
     double* rec = h->rec + (size_t)slot * R_COUNT;
     double* sh = h->shells_dev + (size_t)slot * 2 * (h->allkmax + 1);
-    cudaError_t e = launch_spectra(h, rec, sh);
+    cudaError_t e = launch_spectra(h, rec, sh, (unsigned int)slot + 1u);
     if (e != cudaSuccess) return e;
     if (h->p.timemethod == 1) {
         // the statistics' partials (first stage) stay untouched until the forcing kernel sums them
@@ -762,24 +242,11 @@ cudaError_t flush_pending_scale(bastr_handle* h) {
 
 // Physical <-> truncated spectral state, always in FP64.
 cudaError_t to_spectral(bastr_handle* h) {
-    cudaError_t e;
-    if (h->g.d == 2) {
-        e = l2_xpass<double, XM_FROM_PHYS>(h, nullptr, 0, h->mb, h->phys, nullptr, nullptr);
-        if (e != cudaSuccess) return e;
-        StageIO<double> io{h->u0, nullptr, nullptr, nullptr};
-        return l2_yfwd<double, EPI_STORE>(h, h->mb, io, 0);
-    }
-    return state3d_to_spectral(h);
+    return h->g.d == 2 ? state2d_to_spectral(h) : state3d_to_spectral(h);
 }
 
 cudaError_t to_physical(bastr_handle* h) {
-    cudaError_t e;
-    if (h->g.d == 2) {
-        e = l2_yinv<double, double, YI_STATE>(h, h->u0, h->ma, 2);
-        if (e != cudaSuccess) return e;
-        return l2_xpass<double, XM_TO_PHYS>(h, h->ma, 2, nullptr, nullptr, h->phys, nullptr);
-    }
-    return state3d_to_physical(h);
+    return h->g.d == 2 ? state2d_to_physical(h) : state3d_to_physical(h);
 }
 
 }  // namespace
@@ -1024,20 +491,60 @@ void decode_records(const bastr_handle* h, const double* rec, int nsteps, bastr_
 }
 
 // Launches nsteps steps on the handle's stream into record slots 0..nsteps-1 and advances the
-// host counters.
+// host counters.  The batch's stop word is cleared first; the kernels of the batch see it through
+// h->g.halt, which is set only while they are launched (calls outside a batch, such as the state
+// read-back after a NaN stop, must not skip).
 cudaError_t launch_batch(bastr_handle* h, int nsteps) {
     h->batch_n0 = h->nstep;
     h->batch_t0 = h->time;
-    for (int i = 0; i < nsteps; ++i) {
+    unsigned int* halt = h->done + T_HALT;
+    cudaError_t e = cudaMemsetAsync(halt, 0, sizeof(unsigned int), h->stream);
+    if (e != cudaSuccess) return e;
+    h->g.halt = halt;
+    for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
         const int64_t n = h->nstep;
         const bool vg = h->p.velgrad_every > 0 && (n % h->p.velgrad_every) == 0;
-        cudaError_t e = launch_step(h, i, vg);
-        if (e != cudaSuccess) return e;
+        e = launch_step(h, i, vg);
+        if (e != cudaSuccess) break;
         h->nstep += 1;
         h->time = h->time + h->p.deltat;
     }
+    h->g.halt = nullptr;
+    if (e != cudaSuccess) return e;
     h->chunk_used = nsteps;
     return cudaSuccess;
+}
+
+// After a batch whose stop word read `halt` (0: ran to the end; else the slot + 1 of the step
+// whose Es+Ed was NaN): winds the host counters back to that step, as the reference stops before
+// its nstep = nstep + 1 (solution.F90:81-84), and keeps only the records up to it.  Returns the
+// number of valid records.
+int apply_halt(bastr_handle* h, unsigned int halt, int nsteps) {
+    if (halt == 0 || (int)halt > nsteps) return nsteps;
+    const int k = (int)halt - 1;
+    h->nstep = h->batch_n0;
+    h->time = h->batch_t0;
+    for (int i = 0; i < k; ++i) {
+        h->nstep += 1;
+        h->time = h->time + h->p.deltat;
+    }
+    h->chunk_used = k + 1;
+    return k + 1;
+}
+
+// Records from slot `valid` on belong to steps that did not run after a NaN stop: NaN values.
+void blank_records(bastr_step_out* out, int valid, int nsteps) {
+    if (!out) return;
+    for (int i = valid; i < nsteps; ++i) {
+        bastr_step_out& o = out[i];
+        const int64_t n = out[valid - 1].nstep;
+        const double t = out[valid - 1].time;
+        o.nstep = n;
+        o.time = t;
+        o.Esspe = o.Edspe = o.k2Edspe = o.kMEdspe = NAN;
+        for (double& v : o.velgrad) v = NAN;
+        o.factor = o.E = o.energy = o.Fen = NAN;
+    }
 }
 
 }  // namespace
@@ -1062,15 +569,28 @@ int bastr_step_async(bastr_handle* h, int32_t nsteps) {
 
 int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells) {
     if (!h) return BASTR_E_INVALID;
-    if (nsteps > h->chunk_used) return fail(h, BASTR_E_INVALID, "only %d records available", h->chunk_used);
+    if (nsteps < 0 || nsteps > h->chunk_used) return fail(h, BASTR_E_INVALID, "only %d records available", h->chunk_used);
     CK(cudaSetDevice(h->device));
     std::vector<double> rec((size_t)nsteps * R_COUNT);
+    unsigned int halt = 0;
     if (nsteps) CK(cudaMemcpyAsync(rec.data(), h->rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (shells && nsteps)
         CK(cudaMemcpyAsync(shells, h->shells_dev, (size_t)nsteps * 2 * (h->allkmax + 1) * sizeof(double),
                            cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&halt, h->done + T_HALT, sizeof halt, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    decode_records(h, rec.data(), nsteps, out);
+    // the stop word belongs to the last batch (chunk_used steps); a NaN step within the records asked for
+    const int valid = apply_halt(h, halt, h->chunk_used);
+    const int nv = std::min(valid, (int)nsteps);
+    decode_records(h, rec.data(), nv, out);
+    if (nv < nsteps) {
+        blank_records(out, nv, nsteps);
+        if (shells)
+            std::fill(shells + (size_t)nv * 2 * (h->allkmax + 1), shells + (size_t)nsteps * 2 * (h->allkmax + 1),
+                      (double)NAN);
+    }
+    if (halt != 0 && (int)halt <= nsteps)
+        return fail(h, BASTR_E_NAN, "\"E\" is a NaN at nstep %lld", (long long)(h->batch_n0 + (int)halt - 1));
     return BASTR_OK;
 }
 
@@ -1084,13 +604,16 @@ int bastr_step(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* she
         if (r) return r;
         r = bastr_step_records(h, n, out ? out + done : nullptr,
                                shells ? shells + (size_t)done * 2 * (h->allkmax + 1) : nullptr);
-        if (r) return r;
-        for (int i = 0; i < n && out; ++i) {
-            const bastr_step_out& o = out[done + i];
-            if (std::isnan(o.Esspe + o.Edspe)) {
-                return fail(h, BASTR_E_NAN, "\"E\" is a NaN at nstep %lld", (long long)o.nstep);
-            }
+        if (r == BASTR_E_NAN) {
+            // the records after the NaN step, in this chunk and the ones not run, are NaN
+            const int valid = h->chunk_used;
+            blank_records(out ? out + done : nullptr, valid, nsteps - done);
+            if (shells)
+                std::fill(shells + (size_t)(done + valid) * 2 * (h->allkmax + 1),
+                          shells + (size_t)nsteps * 2 * (h->allkmax + 1), (double)NAN);
+            return r;
         }
+        if (r) return r;
         done += n;
     }
     return BASTR_OK;
@@ -1104,7 +627,7 @@ int bastr_spectra(bastr_handle* h, double* kn, double* Es, double* Ed, int64_t* 
     // use the last chunk slot as scratch
     double* rec = h->rec + (size_t)(kChunk - 1) * R_COUNT;
     double* sh = h->shells_dev + (size_t)(kChunk - 1) * 2 * (am + 1);
-    CK(launch_spectra(h, rec, sh));
+    CK(launch_spectra(h, rec, sh, 0u));
     std::vector<double> buf(2 * (am + 1));
     CK(cudaMemcpyAsync(buf.data(), sh, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));

@@ -101,7 +101,8 @@ __device__ __forceinline__ void spectra_mode(double2* __restrict__ U0, const Geo
 template <int NT>
 __device__ __forceinline__ void spectra_finish(const double* item_part, const int* __restrict__ shell_item,
                                                int nshell, int allkmax, double* __restrict__ rec,
-                                               double* __restrict__ shells_out, double* scratch) {
+                                               double* __restrict__ shells_out, double* scratch,
+                                               unsigned int* halt, unsigned int halt_code) {
     double acc[4] = {0, 0, 0, 0};
     for (int s = threadIdx.x; s < nshell; s += NT) {
         double sh[4] = {0, 0, 0, 0};
@@ -128,6 +129,8 @@ __device__ __forceinline__ void spectra_finish(const double* item_part, const in
         rec[R_ED] = acc[1];
         rec[R_K2ED] = acc[2];
         rec[R_KMED] = acc[3];
+        // solution.F90:69-81: a NaN energy stops the run with this step's state and counters
+        if (halt && halt_code && isnan(acc[0] + acc[1])) *halt = halt_code;
     }
 }
 
@@ -143,8 +146,9 @@ __global__ void __launch_bounds__(NT) k_spectra_fused(double2* __restrict__ U0, 
                                                       double* item_part /* [items][4] */,
                                                       unsigned int* done, const int* __restrict__ shell_item,
                                                       int nshell, int allkmax, double* __restrict__ rec,
-                                                      double* __restrict__ shells_out) {
+                                                      double* __restrict__ shells_out, unsigned int halt_code) {
     pdl_wait();
+    if (halted(g)) return;
     __shared__ double scratch[4 * NT];
     __shared__ unsigned int flag;
     constexpr int U = 4;
@@ -184,7 +188,7 @@ __global__ void __launch_bounds__(NT) k_spectra_fused(double2* __restrict__ U0, 
         for (int i = 0; i < 4; ++i) item_part[(size_t)blockIdx.x * 4 + i] = acc[i];
     }
     if (!last_block_arrives(done, &flag)) return;
-    spectra_finish<NT>(item_part, shell_item, nshell, allkmax, rec, shells_out, scratch);
+    spectra_finish<NT>(item_part, shell_item, nshell, allkmax, rec, shells_out, scratch, g.halt, halt_code);
     if (threadIdx.x == 0) {
         *done = 0;
         pend[0].x = 0.0;   // every block has read it
@@ -197,10 +201,12 @@ template <int NT>
 __global__ void __launch_bounds__(NT) k_spectra_items_final(const double* __restrict__ item_part,
                                                             const int* __restrict__ shell_item, int nshell,
                                                             int allkmax, double* __restrict__ rec,
-                                                            double* __restrict__ shells_out, double2* pend) {
+                                                            double* __restrict__ shells_out, double2* pend,
+                                                            Geo g, unsigned int halt_code) {
     pdl_wait();
+    if (halted(g)) return;
     __shared__ double scratch[4 * NT];
-    spectra_finish<NT>(item_part, shell_item, nshell, allkmax, rec, shells_out, scratch);
+    spectra_finish<NT>(item_part, shell_item, nshell, allkmax, rec, shells_out, scratch, g.halt, halt_code);
     if (threadIdx.x == 0) pend[0].x = 0.0;
 }
 
@@ -253,6 +259,7 @@ template <int NT>
 __global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__ part, int nblk,
                                                       Geo g, double* __restrict__ rec) {
     pdl_wait();
+    if (halted(g)) return;
     __shared__ double scratch[7 * NT];
     velgrad_finish<NT>(part, nblk, g, rec, scratch);
 }
@@ -260,8 +267,9 @@ __global__ void __launch_bounds__(NT) k_velgrad_final(const double* __restrict__
 // Sum of per-block partials in fixed order -> rec[slot] (scaled).
 template <int NT>
 __global__ void __launch_bounds__(NT) k_sum_partials(const double* __restrict__ part, int n, double scale,
-                                                     double* __restrict__ rec, int slot) {
+                                                     double* __restrict__ rec, int slot, Geo g) {
     pdl_wait();
+    if (halted(g)) return;
     __shared__ double scratch[NT];
     double acc[1] = {0};
     for (int b = threadIdx.x; b < n; b += NT) acc[0] += part[b];
@@ -280,6 +288,7 @@ __global__ void __launch_bounds__(NT) k_force_linear(const double* __restrict__ 
                                                      double* __restrict__ rec, double target, double2* pend,
                                                      const double* __restrict__ vg_part, int vg_nblk, Geo g) {
     pdl_wait();
+    if (halted(g)) return;
     __shared__ double scratch[7 * NT];
     if (vg_nblk > 0) {
         velgrad_finish<NT>(vg_part, vg_nblk, g, rec, scratch);
@@ -348,6 +357,7 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
                                                    unsigned long long* rng, const double* __restrict__ vg_part,
                                                    int vg_nblk) {
     pdl_wait();
+    if (halted(g)) return;
     __shared__ double scratch[7 * NT];
     if (vg_nblk > 0) {   // the step's velocity-gradient statistics, as k_force_linear does
         velgrad_finish<NT>(vg_part, vg_nblk, g, rec, scratch);

@@ -25,6 +25,7 @@ struct bastr_ensemble {
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join;
     double* host_rec = nullptr;   // pinned [n_real][kChunk][R_COUNT]
+    unsigned int* host_halt = nullptr;   // pinned [n_real]: each realization's stop word after the batch
     cudaGraphExec_t exec = nullptr;
     int exec_steps = 0;
     std::string err;
@@ -73,6 +74,9 @@ int capture(bastr_ensemble* e, int nsteps) {
         if (st == cudaSuccess)
             st = cudaMemcpyAsync(e->host_rec + i * (size_t)kChunk * R_COUNT, h->rec,
                                  (size_t)nsteps * R_COUNT * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (st == cudaSuccess)
+            st = cudaMemcpyAsync(e->host_halt + i, h->done + T_HALT, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                 h->stream);
         if (st == cudaSuccess) st = cudaEventRecord(e->join[i], h->stream);
         if (st == cudaSuccess) st = cudaStreamWaitEvent(e->main, e->join[i], 0);
     }
@@ -102,9 +106,11 @@ int run_graph(bastr_ensemble* e, int nsteps) {
     return BASTR_OK;
 }
 
-// Host bookkeeping of a replayed batch: counters, records, pending forcing scale.
+// Host bookkeeping of a replayed batch: counters, records, pending forcing scale.  A realization
+// whose stop word is set (a NaN energy) keeps the counters of that step (apply_halt).
 void after_batch(bastr_ensemble* e, int nsteps) {
-    for (bastr_handle* h : e->hs) {
+    for (size_t r = 0; r < e->hs.size(); ++r) {
+        bastr_handle* h = e->hs[r];
         h->batch_n0 = h->nstep;
         h->batch_t0 = h->time;
         for (int i = 0; i < nsteps; ++i) {
@@ -113,6 +119,7 @@ void after_batch(bastr_ensemble* e, int nsteps) {
         }
         h->chunk_used = nsteps;
         if (h->p.forcemethod == 1 && nsteps > 0) h->scale_pending = true;
+        apply_halt(h, e->host_halt[r], nsteps);
     }
 }
 
@@ -145,6 +152,8 @@ int bastr_ensemble_create(const bastr_params* params, int32_t n, bastr_ensemble*
     e->join.resize(n);
     for (int i = 0; i < n; ++i) ECK(cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming));
     ECK(cudaMallocHost(&e->host_rec, (size_t)n * kChunk * R_COUNT * sizeof(double)));
+    ECK(cudaMallocHost(&e->host_halt, (size_t)n * sizeof(unsigned int)));
+    memset(e->host_halt, 0, (size_t)n * sizeof(unsigned int));
     return BASTR_OK;
 }
 
@@ -158,6 +167,7 @@ int bastr_ensemble_destroy(bastr_ensemble* e) {
     if (e->fork) cudaEventDestroy(e->fork);
     if (e->main) cudaStreamDestroy(e->main);
     if (e->host_rec) cudaFreeHost(e->host_rec);
+    if (e->host_halt) cudaFreeHost(e->host_halt);
     delete e;
     return BASTR_OK;
 }
@@ -196,14 +206,13 @@ int bastr_ensemble_step(bastr_ensemble* e, int32_t nsteps, bastr_step_out* out) 
     int status = BASTR_OK;
     for (size_t i = 0; i < e->hs.size(); ++i) {
         bastr_step_out* o = out ? out + i * (size_t)nsteps : nullptr;
-        decode_records(e->hs[i], e->host_rec + i * (size_t)kChunk * R_COUNT, nsteps, o);
-        if (o && status == BASTR_OK) {
-            for (int j = 0; j < nsteps; ++j)
-                if (std::isnan(o[j].Esspe + o[j].Edspe)) {
-                    status = efail(e, BASTR_E_NAN, "realization %zu: \"E\" is a NaN at nstep %lld", i,
-                                   (long long)o[j].nstep);
-                    break;
-                }
+        const int valid = e->hs[i]->chunk_used;   // steps up to a NaN stop
+        decode_records(e->hs[i], e->host_rec + i * (size_t)kChunk * R_COUNT, valid, o);
+        blank_records(o, valid, nsteps);
+        if (valid < nsteps || e->host_halt[i] != 0) {
+            if (status == BASTR_OK)
+                status = efail(e, BASTR_E_NAN, "realization %zu: \"E\" is a NaN at nstep %lld", i,
+                               (long long)e->hs[i]->nstep);
         }
     }
     return status;

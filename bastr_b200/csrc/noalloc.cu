@@ -7,11 +7,13 @@
 // spectra_compute2D/3D (solution.F90:930-1108) on their own arrays.  Its only workspace, the
 // per-shell partial sums, lives in the file-scope device array g_noalloc_shell below, of fixed
 // size: every GPU that loads the library holds those 128 KiB until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <vector>
 
 #include "../../include/bastr_gpu.h"
 #include "solver.cuh"
@@ -29,23 +31,71 @@ constexpr int kMaxDevices = 64;
 // cudaGetSymbolAddress (noalloc_scratch below) and is what the kernels receive.
 static __device__ __align__(256) double g_noalloc_shell[kNoallocMaxShells * 4];
 
-std::mutex g_mu;
-double* g_scratch[kMaxDevices] = {};
+// The address is valid only in the CUDA context that resolved it: another context on the same
+// device (one a driver-API or CUDA Fortran caller made current, or the primary context created
+// anew after a cudaDeviceReset) has its own copy of the array.  So the cache is keyed on the
+// context's unique id (cuCtxGetId, reached through cudaGetDriverEntryPoint so the library needs
+// no link to libcuda), and an address is looked up again in a context not seen before.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 
-// Device address of g_noalloc_shell on the current device, resolved once per device.
+struct ScratchEntry {
+    unsigned long long ctx_id;
+    double* ptr;
+};
+
+std::mutex g_mu;
+std::vector<ScratchEntry> g_scratch;
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+bool g_ctx_fns_tried = false;
+
+// Id of the calling thread's current context, or 0 when there is none yet or the driver does
+// not offer the query.  Called with g_mu held.
+unsigned long long current_ctx_id() {
+    if (!g_ctx_fns_tried) {
+        g_ctx_fns_tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_id = reinterpret_cast<CtxGetIdFn>(f);
+    }
+    if (!g_ctx_current || !g_ctx_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+    if (g_ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of g_noalloc_shell in the current context: looked up once per context (every
+// call, when the context cannot be identified).  The lookup is not a stream operation, but the
+// first call in a context should come before any stream capture.
 cudaError_t noalloc_scratch(double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_shell);
-        if (e != cudaSuccess) return e;
-        g_scratch[dev] = static_cast<double*>(p);
+    unsigned long long id = current_ctx_id();
+    if (id != 0) {
+        for (const ScratchEntry& s : g_scratch)
+            if (s.ctx_id == id) {
+                *out = s.ptr;
+                return cudaSuccess;
+            }
     }
-    *out = g_scratch[dev];
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_shell);   // also makes the device's primary context current
+    if (e != cudaSuccess) return e;
+    if (id == 0) id = current_ctx_id();
+    if (id != 0) g_scratch.push_back({id, static_cast<double*>(p)});
+    *out = static_cast<double*>(p);
     return cudaSuccess;
 }
 
@@ -197,8 +247,16 @@ extern "C" BASTR_API int bastr_spectra_noalloc(int32_t ia, int32_t ja, int32_t k
     const double2* u1 = reinterpret_cast<const double2*>(d_u1spe);
     const double2* u2 = reinterpret_cast<const double2*>(d_u2spe);
     const double2* u3 = reinterpret_cast<const double2*>(d == 3 ? d_u3spe : d_u1spe);
-    if (d == 2) k_spectra_full<2><<<nshell, kNoallocThreads, 0, st>>>(u1, u2, u3, g, scratch);
-    else k_spectra_full<3><<<nshell, kNoallocThreads, 0, st>>>(u1, u2, u3, g, scratch);
-    k_spectra_full_final<<<1, kNoallocThreads, 0, st>>>(scratch, nshell, allkmax, d_Es, d_Ed, d_totals);
-    return cudaGetLastError() == cudaSuccess ? BASTR_OK : BASTR_E_CUDA;
+    // launch statuses are taken from the launches themselves, so that an error the caller left
+    // pending in the runtime's last-error state is neither cleared nor blamed on this call
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(kNoallocThreads);
+    cfg.stream = st;
+    cfg.gridDim = dim3(nshell);
+    cudaError_t e = d == 2 ? cudaLaunchKernelEx(&cfg, k_spectra_full<2>, u1, u2, u3, g, scratch)
+                           : cudaLaunchKernelEx(&cfg, k_spectra_full<3>, u1, u2, u3, g, scratch);
+    if (e != cudaSuccess) return BASTR_E_CUDA;
+    cfg.gridDim = dim3(1);
+    e = cudaLaunchKernelEx(&cfg, k_spectra_full_final, (const double*)scratch, nshell, allkmax, d_Es, d_Ed, d_totals);
+    return e == cudaSuccess ? BASTR_OK : BASTR_E_CUDA;
 }

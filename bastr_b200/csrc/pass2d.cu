@@ -144,6 +144,7 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
         tw = d;
     }
     pdl_wait();
+    if (halted(g)) return;
     const int nitems = (K + G - 1) / G;
     const int colbytes = KY * 2 * (int)sizeof(cplx<TIN>);
     auto issue = [&](int item) {
@@ -289,6 +290,7 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
         twf = d + IFFT::TWS_ELEMS;
     }
     pdl_wait();
+    if (halted(g)) return;
     const int K = g.K, NY = g.ny;
     const int nitems = (NY + G - 1) / G;
     auto issue = [&](int item) {
@@ -496,6 +498,7 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
         tw = d;
     }
     pdl_wait();
+    if (halted(g)) return;
     const int K = g.K, KY = g.KY;
     const int nitems = (K + G - 1) / G;
     // columns kx0.. of every row (records of two rows in MB) -> staging [col][y][c]
@@ -632,6 +635,7 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
         twi = d + FFT::TWS_ELEMS;
     }
     pdl_wait();
+    if (halted(g)) return;
     const int K = g.K, KY = g.KY;
     const int nitems = (K + G - 1) / G;
     // columns kx0.. of every row (records of two rows in MB) -> staging [col][y][c]

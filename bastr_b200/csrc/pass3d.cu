@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(ZInv3D<T, TIN, NZ, SET>::NT)
 k3d_zinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Geo g,
          const cplx<T>* __restrict__ tw) {
     pdl_wait();
+    if (halted(g)) return;
     using P = ZInv3D<T, TIN, NZ, SET>;
     using FFT = typename P::FFT;
     constexpr int EPT = P::EPT, UG = P::UG, F = P::F, G = P::G;
@@ -161,6 +162,7 @@ template <typename T, int NY, int SET>
 __global__ void __launch_bounds__(YInv3D<T, NY, SET>::NT)
 k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const cplx<T>* __restrict__ tw) {
     pdl_wait();
+    if (halted(g)) return;
     using P = YInv3D<T, NY, SET>;
     using FFT = typename P::FFT;
     constexpr int EPT = P::EPT, UG = P::UG, F = P::F, FIN = P::FIN, G = P::G;
@@ -289,6 +291,7 @@ __global__ void __launch_bounds__(XPass3D<T, NX, MODE>::NT)
 k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double* __restrict__ phys_in,
           double* __restrict__ phys_out, double* __restrict__ vg_part, Geo g, const cplx<T>* __restrict__ tw) {
     pdl_wait();
+    if (halted(g)) return;
     using P = XPass3D<T, NX, MODE>;
     using IFFT = typename P::IFFT;
     using FFFT = typename P::FFFT;
@@ -503,6 +506,7 @@ template <typename T, int NY>
 __global__ void __launch_bounds__(YFwd3D<T, NY>::NT)
 k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const cplx<T>* __restrict__ tw) {
     pdl_wait();
+    if (halted(g)) return;
     using P = YFwd3D<T, NY>;
     using FFT = typename P::FFT;
     constexpr int EPT = P::EPT, G = P::G;
@@ -581,6 +585,7 @@ template <typename T, int NZ, int EPI>
 __global__ void __launch_bounds__(ZFwd3D<T, NZ>::NT)
 k3d_zfwd(const cplx<T>* __restrict__ MD, StageIO<T> io, int input_is_u0, Geo g, const cplx<T>* __restrict__ tw) {
     pdl_wait();
+    if (halted(g)) return;
     using P = ZFwd3D<T, NZ>;
     using FFT = typename P::FFT;
     constexpr int EPT = P::EPT, NT = P::NT, G = P::G;

@@ -24,7 +24,18 @@ struct Geo {
     long long ps;       // 3D: stride between the component planes of a spectral field (elements)
     double nu, dt;
     double inv_n;       // 1 / (nx*ny*nz)
+    // Stop word of a batch of steps (null outside bastr_step batches): the spectra kernel of a
+    // step whose Es+Ed is NaN stores that step's slot + 1 there (solution.F90:69-81, `stop '"E" is
+    // a NaN'`), and every kernel launched after it in the batch returns without touching data, so
+    // the state stays the one that produced the NaN.
+    unsigned int* halt;
 };
+
+// True when an earlier kernel of the batch found a NaN energy; the same for every thread of the
+// grid (the word is written by a kernel that completed before this one's pdl_wait returned).
+__device__ __forceinline__ bool halted(const Geo& g) {
+    return g.halt != nullptr && *reinterpret_cast<volatile const unsigned int*>(g.halt) != 0u;
+}
 
 // truncated index -> wavenumber
 __device__ __forceinline__ int trunc_k(int i, int K, int KT) { return i < K ? i : i - KT; }

@@ -64,13 +64,22 @@ def survey_bytes(w, prec):
 # clocks sampled during the timed region
 # -------------------------------------------------------------------------------------------
 class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples (every 100 ms) around the timed region.
+
+    A reader thread time-stamps every line as it arrives, so the samples taken while the GPU was
+    loaded (between ``load_begin`` and ``load_end``) can be told apart from the start-up ones.
+    ``wait_ready`` blocks until the first sample arrived, so that the loaded window is sampled."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.lines = []            # (time, fields)
+        self.t_load = [None, None]
+        self.thread = None
 
     def start(self):
         try:
@@ -79,32 +88,61 @@ class ClockSampler:
                  "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.lines.append((time.perf_counter(), f))
+
+    def wait_ready(self, timeout=5.0):
+        t0 = time.perf_counter()
+        while self.proc and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.02)
+
+    def loaded_samples(self):
+        a, b = self.t_load
+        if a is None:
+            return 0
+        b = b if b is not None else time.perf_counter()
+        return sum(1 for t, _ in self.lines if a <= t <= b)
+
+    def load_begin(self):
+        self.t_load[0] = time.perf_counter()
+
+    def load_end(self):
+        self.t_load[1] = time.perf_counter()
 
     def stop(self):
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-            out = ""
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+        if self.thread:
+            self.thread.join(timeout=2)
+        a, b = self.t_load
+        sm, mx, pw, reasons = [], [], [], set()
+        for t, f in self.lines:
+            if a is not None and b is not None and not (a <= t <= b):
                 continue
             try:
                 sm.append(float(f[1]))
                 mx.append(float(f[2]))
+                pw.append(float(f[3]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
+            for nm, v in zip(self.NAMES, f[5:9]):
                 if v.lower() in ("active", "1", "yes"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "power_w_max": max(pw) if pw else None, "samples": len(sm), "reasons": sorted(reasons),
+                "window": "samples taken while the solver stepped, the timed steps inside the window"}
 
 
 # -------------------------------------------------------------------------------------------
@@ -151,7 +189,19 @@ def device_time(s, stream, nsteps, dist_ctx=None):
     return ms
 
 
+def keep_loaded(s, seconds, chunk=20):
+    """Untimed steps for about `seconds` of wall time (keeps the GPU loaded around the timed
+    region while the clock sampler runs)."""
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        run_steps(s, chunk)
+        s.sync()
+
+
 def measure(wl, prec, steps, warmup, device, dist_ctx=None, sampler=None):
+    """W untimed warm-up steps, then exactly `steps` timed steps.  With a clock sampler the GPU is
+    kept loaded by untimed steps for about 0.6 s before and after the timed region (the same steps
+    as the warm-up), so that the samples under load cover it even when it is a few milliseconds."""
     import torch
     s = make_solver(wl, prec, device)
     u = initial_field(wl)
@@ -162,8 +212,18 @@ def measure(wl, prec, steps, warmup, device, dist_ctx=None, sampler=None):
     s.sync()
     if sampler:
         sampler.start()
+        sampler.wait_ready()
+        sampler.load_begin()
+        keep_loaded(s, 0.6)
     ms = device_time(s, stream, steps, dist_ctx)
-    clocks = sampler.stop() if sampler else None
+    clocks = None
+    if sampler:
+        t0 = time.perf_counter()
+        keep_loaded(s, 0.6)
+        while sampler.loaded_samples() < 10 and time.perf_counter() - t0 < 3.0:
+            keep_loaded(s, 0.1)
+        sampler.load_end()
+        clocks = sampler.stop()
     info = s.info()
     return s, u, stream, ms, clocks, info
 
@@ -188,6 +248,9 @@ def kernel_roofline(s, nsteps, peak, peak_kind, wl, prec):
     return {"kernel": top["name"], "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs",
             "algorithmic_bytes_per_launch": top["bytes_per_launch"], "traffic": traffic,
+            "traffic_source": ("profiles/dram_traffic.json: ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                               "per launch from a capture of this kernel, not measured in this run")
+            if traffic is not None else None,
             "share_of_step": round(top["total_ms"] / total, 4)}, shares
 
 
@@ -300,9 +363,7 @@ def e2e_measure(wl, prec, steps, device):
                     "field uploaded from pinned memory once and downloaded once per timed run"}
 
 
-def cpu_baseline(wl, max_seconds=20.0):
-    """The FP64 c2c CPU oracle on the host cores, on a bounded sample of the same workload."""
-    import numpy as np
+def oracle_for(wl):
     from oracle.bastr_oracle import Oracle, Params
     w = WORKLOADS[wl]
     p = Params(ia=w["ia"], ja=w["ja"], ka=w["ka"], ref_tem=w["ref_tem"], reynolds=w["reynolds"],
@@ -311,6 +372,12 @@ def cpu_baseline(wl, max_seconds=20.0):
     cores = os.cpu_count() or 1
     o = Oracle(p, initial_field(wl), workers=cores)
     o.initial_dealias()
+    return o, cores
+
+
+def cpu_baseline(wl, max_seconds=20.0):
+    """The FP64 c2c CPU oracle on the host cores, on a bounded sample of the same workload."""
+    o, cores = oracle_for(wl)
     t = time.perf_counter()
     o.step_once(True)   # warm-up (plans, page-in)
     first = time.perf_counter() - t
@@ -398,6 +465,9 @@ def ours(args):
                                                            / (peak * 1e9), 4),
                              "dominant_kernel": vroof})
     e2e = e2e_measure(wl, prec, max(20, min(args.steps, 200)), device) if (rank == 0 and not args.no_e2e) else None
+    # the same end-to-end measure in the FP64 form, the reference's own precision
+    e2e64 = (e2e_measure(wl, "fp64", max(20, min(args.steps, 200)), device)
+             if (rank == 0 and not args.no_e2e and prec != "fp64") else None)
     ens = (ensemble_measure(device) if (rank == 0 and n_gpus == 1 and not args.no_variants and not args.no_ensemble)
            else None)
     base = cpu_baseline(wl) if (rank == 0 and n_gpus == 1 and not args.no_cpu) else None
@@ -422,7 +492,7 @@ def ours(args):
         "mpoint_steps_per_s": round(steps_per_s * npts / 1e6, 1),
         "survey_roofline_frac": round(survey_bytes(w, prec) / (ms / args.steps * 1e-3) / (peak * 1e9), 4),
         "roofline": roof, "kernel_shares": shares, "variants": variants, "ensemble": ens,
-        "cpu_baseline": base, "e2e": e2e,
+        "cpu_baseline": base, "e2e": e2e, "e2e_fp64": e2e64,
         "fp32_vs_fp64_rel_l2": acc,
         "gpu_launches": int(info["launches_per_step"] * args.steps),
         "clocks": clocks,
@@ -430,14 +500,35 @@ def ours(args):
     print(json.dumps(line), flush=True)
 
 
-def reference(args):
+def reference(args, budget_s=150.0):
+    """The reference arm: the FP64 c2c CPU restatement of the reference's path (the Fortran
+    reference cannot be built: no Fortran compiler, MPI, FFTW or HDF5), all host cores, on the
+    headline workload.  Each step is one full main-loop step.  Exactly `--warmup` untimed and
+    `--steps` timed steps run when they fit the time budget; otherwise fewer, and the line reports
+    the counts that actually ran."""
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
     wl, _ = HEADLINE
-    base = cpu_baseline(wl, max_seconds=60.0)
+    o, cores = oracle_for(wl)
+    t = time.perf_counter()
+    o.step_once(True)                       # the first warm-up step (plans, page-in)
+    first = time.perf_counter() - t
+    fit = max(2, int(budget_s / max(first, 1e-3)))
+    warmup = max(1, min(args.warmup, fit // 5))
+    steps = max(1, min(args.steps, fit - warmup))
+    for _ in range(warmup - 1):
+        o.step_once(True)
+    t = time.perf_counter()
+    for _ in range(steps):
+        o.step_once(True)
+    dt = time.perf_counter() - t
+    value = round(steps / dt, 5)
+    base = {"value": value, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} full steps of {wl} after {warmup} warm-up steps (FP64 complex-to-complex "
+                      f"restatement, scipy.fft workers={cores})"}
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "steps/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
             "ms_per_step": round(1000.0 / base["value"], 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian field, numpy PCG64 seed 0)",
             "config": {"workload": WORKLOADS[wl]["desc"],

@@ -67,7 +67,7 @@ typedef struct bastr_params {
     double deltat;
     int32_t kmax;                /* allkmax = min(ia/3, kmax) */
     int32_t timemethod;          /* 1 = RK3 (Kutta), 2 = Crank-Nicolson 6-sweep fixed point */
-    int32_t forcemethod;         /* 0 none, 1 linear, 2 band, 5 band to target (3/4: unsupported) */
+    int32_t forcemethod;         /* 0 none, 1 linear, 2 band, 3/4 random-phase band, 5 band to target */
     int32_t forcek;
     double target_energy;
     int32_t lprojectd;           /* project the right-hand side on its dilatational part */
@@ -99,12 +99,16 @@ BASTR_API int bastr_set_counters(bastr_handle* h, int64_t nstep, double time);
 BASTR_API int bastr_get_counters(bastr_handle* h, int64_t* nstep, double* time);
 
 /* Runs nsteps iterations; out[nsteps] (may be NULL); shells (may be NULL) receives, per step,
- * Es[0..allkmax] then Ed[0..allkmax].  Returns BASTR_E_NAN at the first step whose Es+Ed is NaN
- * (that step's record is filled; the state is the one that produced the NaN). */
+ * Es[0..allkmax] then Ed[0..allkmax].  Returns BASTR_E_NAN at the first step whose Es+Ed is NaN,
+ * as the reference stops there (solution.F90:69-81), also when out is NULL: that step's record is
+ * filled, the records and shells of the later steps are NaN, no kernel of a later step runs, and
+ * the state and the counters (bastr_get_state, bastr_get_counters) are those of the NaN step, the
+ * state the reference dumps before it stops. */
 BASTR_API int bastr_step(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells);
 
 /* Enqueues nsteps iterations on the handle's stream and returns without synchronising;
- * per-step records stay on the device (bastr_step_records copies the last batch). */
+ * per-step records stay on the device (bastr_step_records copies the last batch, and returns
+ * BASTR_E_NAN with the counters wound back to the NaN step when the batch stopped at one). */
 BASTR_API int bastr_step_async(bastr_handle* h, int32_t nsteps);
 BASTR_API int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells);
 
@@ -164,7 +168,10 @@ BASTR_API int bastr_profile(bastr_handle* h, int32_t nsteps, bastr_kernel_stat* 
  * The only workspace is a fixed 128 KiB device array inside the library (BASTR_NOALLOC_MAX_SHELLS
  * shells x 4 doubles), held by every GPU that loads the library until the process exits; grids
  * with nint(|k|max) + 1 > BASTR_NOALLOC_MAX_SHELLS are rejected with BASTR_E_TOO_LARGE.  The first
- * call on a device looks up that array's device address, so make it before any stream capture.
+ * call in a CUDA context looks up that array's device address in that context (the address is
+ * cached per context id, so a context made current by the caller, or the primary context created
+ * anew after a cudaDeviceReset, gets its own lookup); make that first call before any stream
+ * capture.
  * All calls share the array: calls that overlap on the GPU (other streams or host threads) race
  * and must be serialised by the caller.  Each call writes every slot it reads, so no clearing is
  * needed between calls.  Runs on `stream` (NULL: legacy default stream), does not synchronise. */

@@ -51,3 +51,30 @@ def test_gpu_matches_fixture(gpu_lib, name, precision):
         assert rel_l2(got[:, j], ref[:, j]) <= col_tol, (j, got[:, j], ref[:, j])
     am = g["shells"].shape[-1]
     assert rel_l2(shells[:, :, :am], g["shells"]) <= tol
+
+
+@pytest.mark.parametrize("name", ["2d2048", "3d256"])
+def test_fullsize_fixture_is_consistent(name):
+    """The frozen full-size oracle runs (tests/golden/make_fullsize.py): the seeded field they
+    started from is the one the generator rebuilds here, and the step-1 record agrees with the
+    oracle's first spectra on that field (the spectra need no time step, so they are cheap)."""
+    from bastr_b200.initfield import seeded_field
+    from oracle.bastr_oracle import Oracle, Params
+    from tests.golden.make_fullsize import CASES as FS
+    path = os.path.join(HERE, f"fullsize_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"fullsize_{name}.npz not generated yet")
+    g = load(f"fullsize_{name}")
+    cfg = FS[name]
+    p = Params(**cfg["params"])
+    u = seeded_field(p.ia, p.ja, p.ka, k0=cfg["k0"], seed=0)
+    assert rel_l2([float(np.sum(c * c)) for c in u], g["u0_sumsq"]) <= 1e-13
+    assert g["records"].shape == (int(g["nsteps"]), 14)
+    assert g["shells"].shape[0] == len(g["shell_steps"])
+    o = Oracle(p, u)
+    o.initial_dealias()
+    sp = o.spectra_compute([o.fft(c) for c in o.u])
+    ref = g["records"][0]
+    for j, key in enumerate(("Esspe", "Edspe", "k2Edspe", "kMEdspe")):
+        assert abs(sp[key] - ref[j]) <= 1e-13 * abs(ref[j])
+    assert rel_l2(sp["Es"], g["shells"][0, 0]) <= 1e-13

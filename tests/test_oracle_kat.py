@@ -294,3 +294,27 @@ def test_hitgen_uniform_stream():
     assert np.array_equal(a, hitgen_uniform(p, 0, 5))
     assert a.min() > 0.0 and a.max() < 1.0 and abs(a.mean() - 0.5) < 0.02
     assert not np.array_equal(a, b) and not np.array_equal(a, c)
+
+
+def test_nan_energy_stops_before_the_step_advances():
+    """solution.F90:69-84: a NaN Es+Ed dumps the field of that step and stops before nstep and
+    time advance, so the dumped state is the one that produced the NaN."""
+    import warnings
+
+    from bastr_b200.initfield import seeded_field
+    p = Params(ia=32, ja=32, ka=0, reynolds=0.0, deltat=0.03, forcemethod=2, forcek=3, target_energy=200.0,
+               kmax=10)
+    o = Oracle(p, [10.0 * c for c in seeded_field(32, 32, 0, k0=3.0, seed=5)], workers=1)
+    o.initial_dealias()
+    n_ok = 0
+    with np.errstate(all="ignore"), warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        with pytest.raises(FloatingPointError):
+            for _ in range(20):
+                o.step_once(True)
+                n_ok += 1
+    assert o.nstep == n_ok and n_ok >= 2
+    assert o.time == pytest.approx(n_ok * p.deltat)
+    fnum, nstep, time, dumped = o.dumps[-1]
+    assert nstep == o.nstep
+    assert all(a is not b and np.array_equal(a, b, equal_nan=True) for a, b in zip(dumped, o.u))

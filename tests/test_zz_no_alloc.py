@@ -28,13 +28,16 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.mark.parametrize("dims", [(64, 64, 0), (64, 128, 0), (32, 32, 32)], ids=["2d", "2d_rect", "3d"])
-def test_noalloc_spectra_match_handle(gpu_lib, dims):
+@pytest.mark.parametrize("dims,kmax", [((64, 64, 0), 100), ((64, 128, 0), 100), ((32, 32, 32), 100),
+                                       ((64, 64, 0), 5), ((32, 64, 32), 100), ((16, 32, 64), 3)],
+                         ids=["2d", "2d_rect", "3d", "2d_kmax5", "3d_rect", "3d_rect_kmax3"])
+def test_noalloc_spectra_match_handle(gpu_lib, dims, kmax):
+    """kmax below ia/3 truncates allkmax (the shells past it are not returned, the totals still
+    cover every mode); non-cubic 3D grids have per-axis Nyquist limits."""
     import torch
 
     from bastr_b200 import BASTR_OK, BastrGPU, load_library, seeded_field
     ia, ja, ka = dims
-    kmax = 100
     u = seeded_field(ia, ja, ka, k0=4.0 if ka == 0 else 3.0, seed=11)
     with BastrGPU(ia, ja, ka, kmax=kmax, reynolds=5000.0, deltat=1e-4, precision="fp64") as s:
         s.set_state(u)                   # dealiases, as mainloop does before its first step
@@ -55,15 +58,19 @@ def test_noalloc_spectra_match_handle(gpu_lib, dims):
 
     lib = load_library()
     results = []
-    for _ in range(2):
+    for call in range(2):
         for t in (d_es, d_ed, d_tot):
             t.fill_(math.nan)
         torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(dev)[0]
         rc = lib.bastr_spectra_noalloc(ia, ja, ka, kmax, _ptr(spe[0]), _ptr(spe[1]),
                                        _ptr(spe[2] if ka else spe[0]), _ptr(d_es), _ptr(d_ed),
                                        _ptr(d_tot), None)
         assert rc == BASTR_OK
         torch.cuda.synchronize()
+        if call == 1:
+            # the first call may load the kernels' module; the second allocates no device memory
+            assert torch.cuda.mem_get_info(dev)[0] == free0
         es, ed, tot = d_es.cpu().numpy(), d_ed.cpu().numpy(), d_tot.cpu().numpy()
         assert _rel(es, es_ref) <= TOL
         assert _rel(ed, ed_ref) <= TOL
@@ -73,6 +80,15 @@ def test_noalloc_spectra_match_handle(gpu_lib, dims):
     # the shared workspace keeps the last call's contents; a repeated call gives the same bits
     for a, b in zip(results[0], results[1]):
         assert np.array_equal(a, b)
+    # without the totals array: the shells alone, the same values
+    d_es.fill_(math.nan)
+    d_ed.fill_(math.nan)
+    rc = lib.bastr_spectra_noalloc(ia, ja, ka, kmax, _ptr(spe[0]), _ptr(spe[1]), _ptr(spe[2] if ka else spe[0]),
+                                   _ptr(d_es), _ptr(d_ed), None, None)
+    assert rc == BASTR_OK
+    torch.cuda.synchronize()
+    assert np.array_equal(d_es.cpu().numpy(), results[0][0])
+    assert np.array_equal(d_ed.cpu().numpy(), results[0][1])
 
 
 def test_noalloc_rejects_grids_beyond_its_workspace(gpu_lib):
