@@ -339,6 +339,26 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     dev_alloc(h, &h->rec, (size_t)kChunk * R_COUNT * sizeof(double), st);
     dev_alloc(h, &h->shells_dev, (size_t)kChunk * 2 * (h->allkmax + 1) * sizeof(double), st);
     if (st != cudaSuccess) return fail(h, BASTR_E_CUDA, "device allocation failed: %s", cudaGetErrorString(st));
+    g.err = h->done + T_ERR;
+    if (d == 2) {
+        // TMA tensor maps of the 2D mixed-field buffers (compute precision; see TensorMapSlot)
+        const uint64_t el = cs / 2, RB = 4 * cs, NY = g.ny, KK = K;
+        const uint32_t BK = (uint32_t)std::min(K, 256), BY = (uint32_t)std::min(g.ny / 2, 256);
+        const int swa = (int)RB;                       // 32 (FP32) / 64 (FP64)
+        const int swb = 2 * cs == 32 ? 32 : 0;
+        const uint64_t d4[4] = {8, NY, 1, KK}, s4[3] = {RB, NY * RB, NY * RB};
+        const uint64_t d8[4] = {8, NY, 2, KK}, s8[3] = {RB, NY * RB, 2 * NY * RB};
+        const uint32_t ba[4] = {8, 1, 1, BK}, bb[4] = {4, 1, 1, BK};
+        // MB records of FP32 (32 bytes) and FP64 (64 bytes) values; MB holds the FP64 layout always
+        const uint64_t dy[3] = {8, KK, NY / 2}, sy32[2] = {32, KK * 32}, sy64[2] = {64, KK * 64};
+        const uint32_t by[3] = {8, 1, BY};
+        const bool ok = encode_map(&h->tm[TM_XA4], h->ma, (int)el, 4, d4, s4, ba, swa) &&
+                        encode_map(&h->tm[TM_XA8], h->ma, (int)el, 4, d8, s8, ba, swa) &&
+                        encode_map(&h->tm[TM_XB8], h->ma, (int)el, 4, d8, s8, bb, swb) &&
+                        encode_map(&h->tm[TM_YMB32], h->mb, 4, 3, dy, sy32, by, 0) &&
+                        encode_map(&h->tm[TM_YMB64], h->mb, 8, 3, dy, sy64, by, 64);
+        if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a mixed-field tensor map");
+    }
 
     const int ns[3] = {g.nx, g.ny, d == 3 ? g.nz : 0};
     for (int a = 0; a < 3; ++a) {
@@ -572,13 +592,19 @@ int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, dou
     if (nsteps < 0 || nsteps > h->chunk_used) return fail(h, BASTR_E_INVALID, "only %d records available", h->chunk_used);
     CK(cudaSetDevice(h->device));
     std::vector<double> rec((size_t)nsteps * R_COUNT);
-    unsigned int halt = 0;
+    unsigned int words[2] = {0, 0};   // the batch's stop word and the kernels' error word
     if (nsteps) CK(cudaMemcpyAsync(rec.data(), h->rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (shells && nsteps)
         CK(cudaMemcpyAsync(shells, h->shells_dev, (size_t)nsteps * 2 * (h->allkmax + 1) * sizeof(double),
                            cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(&halt, h->done + T_HALT, sizeof halt, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(words, h->done + T_HALT, sizeof words, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    const unsigned int halt = words[0];
+    if (words[1] != 0) {
+        CK(cudaMemsetAsync(h->done + T_ERR, 0, sizeof(unsigned int), h->stream));
+        return fail(h, BASTR_E_CUDA, "a kernel of the last batch gave up waiting for its TMA staging (error word %u)",
+                    words[1]);
+    }
     // the stop word belongs to the last batch (chunk_used steps); a NaN step within the records asked for
     const int valid = apply_halt(h, halt, h->chunk_used);
     const int nv = std::min(valid, (int)nsteps);

@@ -3,6 +3,7 @@
 // step schedules (steps2d.cuh, steps3d.cuh) are compiled in their own translation units, one per
 // compute precision, so that the library builds in parallel; capi.cu holds the C ABI.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,6 +34,7 @@
         if (le_ != cudaSuccess) return le_;         \
     } while (0)
 #include "solver.cuh"
+#include "tma.cuh"
 
 using namespace bastr;
 
@@ -111,12 +113,61 @@ struct bastr_handle {
     std::vector<ProfRec> prof;
     std::vector<double> kn;
     std::vector<int64_t> ecount;
+    // TMA tensor maps of the mixed-field buffers (2D, compute precision), built at creation
+    CUtensorMap tm[5] = {};
 };
 
 namespace bastr_impl {
 
-// Slots of h->done: one per kind of last-block reduction (each stays 0 between launches).
-enum Ticket : int { T_SPECTRA = 0, T_HALT = 1, kTickets = 4 };
+// Slots of h->done: one per kind of last-block reduction (each stays 0 between launches), the
+// batch's stop word and the kernels' error word (Geo::halt, Geo::err).
+enum Ticket : int { T_SPECTRA = 0, T_HALT = 1, T_ERR = 2, kTickets = 4 };
+
+// Tensor maps of a 2D handle (bastr_handle::tm):
+//   TM_XA4 / TM_XA8  MA records [kx][ftot/4][y][4 fields] (ftot 4 / 8), box = 4 fields x 1 row x BK kx
+//   TM_XB8           the (q1, q2) pieces of the second record (ftot 8), box = 2 fields x 1 row x BK kx
+//   TM_YMB32/64      MB records [y/2][kx][2 rows][2 comps] in FP32 / FP64, box = 4 values x 1 kx x
+//                    BY row pairs (the FP64 one also serves the state transform of FP32 handles)
+enum TensorMapSlot : int { TM_XA4 = 0, TM_XA8 = 1, TM_XB8 = 2, TM_YMB32 = 3, TM_YMB64 = 4, kTensorMaps = 5 };
+
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point (no link to libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+inline EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiledFn) nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+
+// A tiled tensor map of `rank` dimensions over a buffer of this GPU (dims innermost first, in
+// elements of `elem` bytes; strides of dims 1.. in bytes); swizzle in bytes (0, 32, 64, 128).
+// Out-of-range box elements read as zero.  Returns false when the driver rejects it.
+inline bool encode_map(CUtensorMap* m, const void* base, int elem, int rank, const uint64_t* dims,
+                       const uint64_t* strides, const uint32_t* box, int swizzle) {
+    EncodeTiledFn fn = encode_tiled_fn();
+    if (!fn) return false;
+    cuuint64_t gd[5], gs[4];
+    cuuint32_t bx[5], es[5];
+    for (int i = 0; i < rank; ++i) {
+        gd[i] = dims[i];
+        bx[i] = box[i];
+        es[i] = 1;
+        if (i + 1 < rank) gs[i] = strides[i];
+    }
+    const CUtensorMapSwizzle sw = swizzle == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                : swizzle == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                : swizzle == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE;
+    const CUtensorMapDataType dt = elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    return fn(m, dt, (cuuint32_t)rank, const_cast<void*>(base), gd, gs, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 inline int fail(bastr_handle* h, int code, const char* fmt, ...) {
     char buf[512];

@@ -25,6 +25,7 @@
 // the copy of the next group is issued, so it lands while the current group is transformed.
 #include "regfft.cuh"
 #include "solver.cuh"
+#include "tma.cuh"
 
 namespace bastr {
 
@@ -123,6 +124,8 @@ template <typename T, typename TIN, int NY, int SET> struct YInv2D {
     }
     static constexpr size_t TWB = tw_stage_bytes<T, FFT>();
     static size_t smem(int KY) { return stage_bytes(KY) + XCH + TWB; }
+    // one column per block: staged by one bulk copy (TMA, contiguous run) on an mbarrier
+    static constexpr bool TMA = G == 1;
 };
 
 template <typename T, typename TIN, int NY, int SET>
@@ -146,18 +149,44 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
     pdl_wait();
     if (halted(g)) return;
     const int nitems = (K + G - 1) / G;
-    const int colbytes = KY * 2 * (int)sizeof(cplx<TIN>);
+    const int colbytes = KY * 2 * (int)sizeof(cplx<TIN>);   // a multiple of 16
+    __shared__ __align__(8) uint64_t bar;
+    if constexpr (P::TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    uint32_t phase = 0;
+    bool lost = false;   // a TMA completion wait gave up (recorded in g.err)
     auto issue = [&](int item) {
         const int kx0 = item * G;
         const int ncol = min(G, K - kx0);
-        stage_line(stg, S + (size_t)kx0 * KY * 2, ncol * colbytes);
-        cp_async_commit();
+        if constexpr (P::TMA) {
+            if (threadIdx.x == 0) {
+                mbar_expect_tx(&bar, (uint32_t)colbytes);
+                bulk_load(stg, S + (size_t)kx0 * KY * 2, (uint32_t)colbytes, &bar);
+            }
+        } else {
+            stage_line(stg, S + (size_t)kx0 * KY * 2, ncol * colbytes);
+            cp_async_commit();
+        }
     };
     int item = blockIdx.x;
     if (item < nitems) issue(item);
     for (; item < nitems; item += gridDim.x) {
-        cp_async_wait<0>();
-        __syncthreads();
+        if constexpr (P::TMA) {
+            const bool ok = mbar_wait(&bar, phase, g.err);
+            if (__syncthreads_or(!ok)) {   // block-uniform: stop, and drain below
+                lost = true;
+                break;
+            }
+            phase ^= 1u;
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         const cplx<TIN>* col = stg + (size_t)gi * KY * 2;
         const int kx = item * G + gi;
         const bool valid = kx < K;
@@ -212,6 +241,10 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
         }
     }
     cp_async_wait<0>();
+    if constexpr (P::TMA) {
+        if (lost && threadIdx.x == 0) mbar_wait(&bar, phase, nullptr);   // bounded drain
+    }
+    (void)lost;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -247,13 +280,34 @@ template <typename T, int NX, int MODE> struct XPass2D {
     static constexpr int KBASE = (FLIVE < FIN && G == 1) ? FLIVE : FIN * G;
     static constexpr int KPAD = (KBASE * (int)sizeof(cplx<T>) / 16) % 2 == 0 ? 16 / (int)sizeof(cplx<T>) : 0;
     static constexpr int KSTR = KBASE + KPAD;                                // elements per kx
-    static constexpr size_t STAGE = MODE == XM_FROM_PHYS ? (size_t)G * 2 * NX * sizeof(double)
-                                                          : (size_t)KMAX * KSTR * sizeof(cplx<T>);
+    // TMA staging (one row per block, the product modes): tile A holds the records of the four
+    // fields (g1, h1, g2, h2) of every kx, RB bytes each, swizzled at RB bytes so that the threads
+    // of a warp (consecutive kx) read their 16-byte pieces from distinct banks; with velocity-
+    // gradient fields, tile B holds the (q1, q2) pieces (QB bytes each).  Boxes of BK records.
+    static constexpr bool TMA = G == 1 && (MODE == XM_RHS || MODE == XM_RHS_VG);
+    static constexpr int RB = 4 * (int)sizeof(cplx<T>);
+    static constexpr int QB = 2 * (int)sizeof(cplx<T>);
+    static constexpr int SWZA = RB;                     // 32-byte (FP32) or 64-byte (FP64) swizzle
+    static constexpr int SWZB = QB == 32 ? 32 : 0;      // FP64 q pieces: 32-byte swizzle
+    static constexpr int BK = KMAX < 256 ? KMAX : 256;
+    static constexpr int NBOX = (KMAX + BK - 1) / BK;
+    static constexpr size_t TILEA = ((size_t)NBOX * BK * RB + 1023) & ~(size_t)1023;
+    static constexpr size_t TILEB = MODE == XM_RHS_VG ? (((size_t)NBOX * BK * QB + 1023) & ~(size_t)1023) : 0;
+    static constexpr uint32_t TX_BYTES = (uint32_t)(NBOX * BK * (RB + (MODE == XM_RHS_VG ? QB : 0)));
+    static constexpr size_t STAGE = TMA ? 1024 + TILEA + TILEB   // 1024: alignment of the tiles
+                                  : MODE == XM_FROM_PHYS ? (size_t)G * 2 * NX * sizeof(double)
+                                                         : (size_t)KMAX * KSTR * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
     static constexpr size_t TWB = BASTR_XPASS_TW_SMEM ? tw_stage_bytes<T, IFFT, FFFT>() : 0;
     static constexpr size_t SMEM = STAGE + XCHR + TWB;
 };
+
+// 16-byte chunk c of kx record k of a swizzled TMA tile (RB-byte records).
+template <int SWZ, int RB, typename V>
+__device__ __forceinline__ V tile_chunk(const unsigned char* tile, int k, int c) {
+    return *reinterpret_cast<const V*>(tile + swz<SWZ>((uint32_t)(k * RB + c * 16)));
+}
 
 // Packs the half-spectrum values A, B of wavenumber k (0 <= k < K) for one position of a
 // length-NX sequence whose inverse transform is a + i b.  `mirror` selects the position NX-k
@@ -268,13 +322,18 @@ template <typename T, int NX, int MODE>
 __global__ void __launch_bounds__(XPass2D<T, NX, MODE>::NT, XPass2D<T, NX, MODE>::MINB)
 k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
           const double* __restrict__ phys_in, double* __restrict__ phys_out,
-          double* __restrict__ vg_part, Geo g, const cplx<T>* tw) {
+          double* __restrict__ vg_part, Geo g, const cplx<T>* tw,
+          const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB) {
     using P = XPass2D<T, NX, MODE>;
     using IFFT = typename P::IFFT;
     using FFFT = typename P::FFFT;
     constexpr int ZU = P::ZU, EPT = P::EPT, NT = P::NT, NTR = P::NTR, G = P::G, FIN = P::FIN;
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char* stg = smraw;
+    // TMA tiles start at the first 1024-byte boundary of the staging area
+    unsigned char* tileA = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    unsigned char* tileB = tileA + P::TILEA;
+    __shared__ __align__(8) uint64_t bar;
     const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE) + gi * IFFT::SMEM_ELEMS;
     // twiddles by stage in shared memory: the inverse plan (shared by IFFT and IFFTB), then the forward one
@@ -293,10 +352,31 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
     if (halted(g)) return;
     const int K = g.K, NY = g.ny;
     const int nitems = (NY + G - 1) / G;
+    if constexpr (P::TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    uint32_t phase = 0;
     auto issue = [&](int item) {
         const int y0 = item * G;
         const int nrow = min(G, NY - y0);
-        if constexpr (MODE == XM_FROM_PHYS) {
+        if constexpr (P::TMA) {
+            // one thread: the records of row y0 for every kx, as NBOX boxes of BK wavenumbers
+            (void)nrow;
+            if (threadIdx.x == 0) {
+                mbar_expect_tx(&bar, P::TX_BYTES);
+#pragma unroll
+                for (int b = 0; b < P::NBOX; ++b) {
+                    tma_load_4d(tileA + (size_t)b * P::BK * P::RB, &tmA, 0, y0, 0, b * P::BK, &bar);
+                    if constexpr (MODE == XM_RHS_VG)
+                        tma_load_4d(tileB + (size_t)b * P::BK * P::QB, &tmB, 0, y0, 1, b * P::BK, &bar);
+                }
+            }
+            return;
+        } else if constexpr (MODE == XM_FROM_PHYS) {
             double* d = reinterpret_cast<double*>(stg);
             stage_line(d, phys_in + (size_t)y0 * NX, nrow * NX * 8);
             stage_line(d + G * NX, phys_in + (size_t)NY * NX + (size_t)y0 * NX, nrow * NX * 8);
@@ -322,9 +402,19 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
     double divmax = 0.0;
     int item = blockIdx.x;
     if (item < nitems) issue(item);
+    bool lost = false;   // a TMA completion wait gave up (recorded in g.err)
     for (; item < nitems; item += gridDim.x) {
-        cp_async_wait<0>();
-        __syncthreads();
+        if constexpr (P::TMA) {
+            const bool ok = mbar_wait(&bar, phase, g.err);
+            if (__syncthreads_or(!ok)) {   // block-uniform: stop, and drain below
+                lost = true;
+                break;
+            }
+            phase ^= 1u;
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         const int y = item * G + gi;
         const bool valid = y < NY;
         cplx<T> v[ZU * EPT];
@@ -353,19 +443,52 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                     const cplx<T>* src0 = row + (size_t)k * P::KSTR;
                     const bool z0 = p == 0;
                     cplx<T> g1, h1;
-                    ld2<T>(src0, g1, h1);
+                    if constexpr (P::TMA) {
+                        if constexpr (sizeof(T) == 4) {
+                            const float4 q = tile_chunk<P::SWZA, P::RB, float4>(tileA, k, 0);
+                            g1 = mk<T>(q.x, q.y);
+                            h1 = mk<T>(q.z, q.w);
+                        } else {
+                            g1 = tile_chunk<P::SWZA, P::RB, cplx<T>>(tileA, k, 0);
+                            h1 = tile_chunk<P::SWZA, P::RB, cplx<T>>(tileA, k, 1);
+                        }
+                    } else {
+                        ld2<T>(src0, g1, h1);
+                    }
                     if constexpr (MODE == XM_TO_PHYS) {
                         v[e] = pack_at<T>(g1, h1, hi, z0);
                     } else {
                         cplx<T> g2, h2;
-                        ld2<T>(src0 + 2, g2, h2);
+                        if constexpr (P::TMA) {
+                            if constexpr (sizeof(T) == 4) {
+                                const float4 q = tile_chunk<P::SWZA, P::RB, float4>(tileA, k, 1);
+                                g2 = mk<T>(q.x, q.y);
+                                h2 = mk<T>(q.z, q.w);
+                            } else {
+                                g2 = tile_chunk<P::SWZA, P::RB, cplx<T>>(tileA, k, 2);
+                                h2 = tile_chunk<P::SWZA, P::RB, cplx<T>>(tileA, k, 3);
+                            }
+                        } else {
+                            ld2<T>(src0 + 2, g2, h2);
+                        }
                         const T kx = (T)k;
                         v[e] = pack_at<T>(g1, g2, hi, z0);
                         v[EPT + e] = pack_at<T>(cscale<T>(cmuli<T>(g1), kx), cscale<T>(cmuli<T>(g2), kx), hi, z0);
                         v[2 * EPT + e] = pack_at<T>(h1, h2, hi, z0);
                         if constexpr (MODE == XM_RHS_VG) {
                             cplx<T> q1, q2;
-                            ld2<T>(src0 + G * W, q1, q2);
+                            if constexpr (P::TMA) {
+                                if constexpr (sizeof(T) == 4) {
+                                    const float4 q = tile_chunk<P::SWZB, P::QB, float4>(tileB, k, 0);
+                                    q1 = mk<T>(q.x, q.y);
+                                    q2 = mk<T>(q.z, q.w);
+                                } else {
+                                    q1 = tile_chunk<P::SWZB, P::QB, cplx<T>>(tileB, k, 0);
+                                    q2 = tile_chunk<P::SWZB, P::QB, cplx<T>>(tileB, k, 1);
+                                }
+                            } else {
+                                ld2<T>(src0 + G * W, q1, q2);
+                            }
                             const T kx2 = kx * kx;
                             v[3 * EPT + e] = pack_at<T>(csub<T>(cscale<T>(g1, -kx2), q1),
                                                         csub<T>(cscale<T>(g2, -kx2), q2), hi, z0);
@@ -451,6 +574,10 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
         }
     }
     cp_async_wait<0>();
+    if constexpr (P::TMA) {
+        if (lost && threadIdx.x == 0) mbar_wait(&bar, phase, nullptr);   // bounded drain
+    }
+    (void)lost;
     if constexpr (MODE == XM_RHS_VG) {
         __syncthreads();
         double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
@@ -467,13 +594,46 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
 // ---------------------------------------------------------------------------------------
 // Pass C: forward transforms along y of kx columns + spectral epilogue.
 // ---------------------------------------------------------------------------------------
+// TMA staging of the forward y passes (one kx column per block): the column's records of two
+// rows [y/2][2 rows][2 comps] (RB bytes) for every row pair, as NBOX boxes of BY row pairs.  The
+// FP64 records are swizzled at 64 bytes so that the threads of a warp (consecutive y) read their
+// 16-byte pieces from distinct banks; the FP32 ones are read as consecutive 16-byte pieces.
+template <typename T, int NY, int G> struct YStage2D {
+    static constexpr bool TMA = G == 1;
+    static constexpr int RB = 4 * (int)sizeof(cplx<T>);
+    static constexpr int SWZ = RB == 64 ? 64 : 0;
+    static constexpr int NP = NY / 2;
+    static constexpr int BY = NP < 256 ? NP : 256;
+    static constexpr int NBOX = NP / BY;
+    static constexpr uint32_t TX_BYTES = (uint32_t)(NP * RB);
+    static constexpr size_t BYTES = 1024 + (((size_t)NP * RB + 1023) & ~(size_t)1023);
+    // the two components of row y
+    __device__ static __forceinline__ void load(const unsigned char* tile, int y, cplx<T>& a, cplx<T>& b) {
+        if constexpr (sizeof(T) == 4) {
+            const float4 q = *reinterpret_cast<const float4*>(tile + (size_t)y * 16);
+            a = mk<T>(q.x, q.y);
+            b = mk<T>(q.z, q.w);
+        } else {
+            a = *reinterpret_cast<const cplx<T>*>(tile + swz<SWZ>((uint32_t)y * 32));
+            b = *reinterpret_cast<const cplx<T>*>(tile + swz<SWZ>((uint32_t)y * 32 + 16));
+        }
+    }
+    // one thread: column kx of every row pair
+    __device__ static __forceinline__ void issue(unsigned char* tile, const CUtensorMap* map, int kx, uint64_t* bar) {
+        mbar_expect_tx(bar, TX_BYTES);
+#pragma unroll
+        for (int b = 0; b < NBOX; ++b) tma_load_3d(tile + (size_t)b * BY * RB, map, 0, kx, b * BY, bar);
+    }
+};
+
 template <typename T, int NY> struct YFwd2D {
     static constexpr int EPT = ept_fit<NY, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_YFWD_F32>();
     using FFT = RegFFT<T, NY, EPT, 2, false>;
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
     static constexpr int MINB = NT >= 256 ? 2 : 1;
-    static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<T>);
+    using YS = YStage2D<T, NY, G>;
+    static constexpr size_t STAGE = YS::TMA ? YS::BYTES : (size_t)G * NY * 2 * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
     static constexpr size_t TWB = tw_stage_bytes<T, FFT>();
@@ -483,7 +643,7 @@ template <typename T, int NY> struct YFwd2D {
 template <typename T, int NY, int EPI>
 __global__ void __launch_bounds__(YFwd2D<T, NY>::NT, YFwd2D<T, NY>::MINB)
 k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
-         const cplx<T>* tw) {
+         const cplx<T>* tw, const __grid_constant__ CUtensorMap tmy) {
     using P = YFwd2D<T, NY>;
     using FFT = typename P::FFT;
     constexpr int EPT = P::EPT, NT = P::NT, G = P::G;
@@ -501,8 +661,24 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
     if (halted(g)) return;
     const int K = g.K, KY = g.KY;
     const int nitems = (K + G - 1) / G;
+    using YS = typename P::YS;
+    unsigned char* tile = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    __shared__ __align__(8) uint64_t bar;
+    if constexpr (YS::TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    uint32_t phase = 0;
+    bool lost = false;   // a TMA completion wait gave up (recorded in g.err)
     // columns kx0.. of every row (records of two rows in MB) -> staging [col][y][c]
     auto issue = [&](int item) {
+        if constexpr (YS::TMA) {
+            if (threadIdx.x == 0) YS::issue(tile, &tmy, item, &bar);
+            return;
+        }
         const int kx0 = item * G;
         const int ncol = min(G, K - kx0);
         constexpr int C16 = 2 * (int)sizeof(cplx<T>) / 16;
@@ -522,8 +698,17 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
     int item = blockIdx.x;
     if (item < nitems) issue(item);
     for (; item < nitems; item += gridDim.x) {
-        cp_async_wait<0>();
-        __syncthreads();
+        if constexpr (YS::TMA) {
+            const bool ok = mbar_wait(&bar, phase, g.err);
+            if (__syncthreads_or(!ok)) {   // block-uniform: stop, and drain below
+                lost = true;
+                break;
+            }
+            phase ^= 1u;
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         const cplx<T>* col = stg + (size_t)gi * NY * 2;
         const int kx = item * G + gi;
         const bool valid = kx < K;
@@ -531,8 +716,9 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
 #pragma unroll
         for (int e = 0; e < EPT; ++e) {
             const int y = FFT::in_pos(t, e);
-            if (valid) ld2<T>(col + 2 * y, v[e], v[EPT + e]);
-            else v[e] = v[EPT + e] = mk<T>(0, 0);
+            if (!valid) v[e] = v[EPT + e] = mk<T>(0, 0);
+            else if constexpr (YS::TMA) YS::load(tile, y, v[e], v[EPT + e]);
+            else ld2<T>(col + 2 * y, v[e], v[EPT + e]);
         }
         __syncthreads();   // the staging buffer is free: fetch the next column group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
@@ -572,6 +758,10 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
         }
     }
     cp_async_wait<0>();
+    if constexpr (YS::TMA) {
+        if (lost && threadIdx.x == 0) mbar_wait(&bar, phase, nullptr);   // bounded drain
+    }
+    (void)lost;
     if constexpr (EPI == EPI_RK3 || EPI == EPI_CN_LAST) {
         if (io.energy_part) {
             __syncthreads();
@@ -602,7 +792,8 @@ template <typename T, int NY> struct YFwdInv2D {
     static constexpr int G = groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
     static constexpr int MINB = (sizeof(T) == 4 && NT >= 256) ? BASTR_MINB_YFI : 1;
-    static constexpr size_t STAGE = (size_t)G * NY * 2 * sizeof(cplx<T>);
+    using YS = YStage2D<T, NY, G>;
+    static constexpr size_t STAGE = YS::TMA ? YS::BYTES : (size_t)G * NY * 2 * sizeof(cplx<T>);
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)NT * 8 ? XCH : (size_t)NT * 8;
     static constexpr size_t TWB = tw_stage_bytes<T, FFT, IFFT>();
@@ -612,7 +803,7 @@ template <typename T, int NY> struct YFwdInv2D {
 template <typename T, int NY, int EPI>
 __global__ void __launch_bounds__(YFwdInv2D<T, NY>::NT, YFwdInv2D<T, NY>::MINB)
 k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g, const cplx<T>* tw,
-             cplx<T>* __restrict__ MA) {
+             cplx<T>* __restrict__ MA, const __grid_constant__ CUtensorMap tmy) {
     static_assert(EPI == EPI_RK1 || EPI == EPI_RK2 || EPI == EPI_CN_MID, "stages that hand on a stage input");
     using P = YFwdInv2D<T, NY>;
     using FFT = typename P::FFT;
@@ -638,8 +829,24 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
     if (halted(g)) return;
     const int K = g.K, KY = g.KY;
     const int nitems = (K + G - 1) / G;
+    using YS = typename P::YS;
+    unsigned char* tile = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    __shared__ __align__(8) uint64_t bar;
+    if constexpr (YS::TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    uint32_t phase = 0;
+    bool lost = false;   // a TMA completion wait gave up (recorded in g.err)
     // columns kx0.. of every row (records of two rows in MB) -> staging [col][y][c]
     auto issue = [&](int item) {
+        if constexpr (YS::TMA) {
+            if (threadIdx.x == 0) YS::issue(tile, &tmy, item, &bar);
+            return;
+        }
         const int kx0 = item * G;
         const int ncol = min(G, K - kx0);
         constexpr int C16 = 2 * (int)sizeof(cplx<T>) / 16;
@@ -659,8 +866,17 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
     int item = blockIdx.x;
     if (item < nitems) issue(item);
     for (; item < nitems; item += gridDim.x) {
-        cp_async_wait<0>();
-        __syncthreads();
+        if constexpr (YS::TMA) {
+            const bool ok = mbar_wait(&bar, phase, g.err);
+            if (__syncthreads_or(!ok)) {   // block-uniform: stop, and drain below
+                lost = true;
+                break;
+            }
+            phase ^= 1u;
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         const cplx<T>* col = stg + (size_t)gi * NY * 2;
         const int kx = item * G + gi;
         const bool valid = kx < K;
@@ -668,8 +884,9 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
 #pragma unroll
         for (int e = 0; e < EPT; ++e) {
             const int y = FFT::in_pos(t, e);
-            if (valid) ld2<T>(col + 2 * y, v[e], v[EPT + e]);
-            else v[e] = v[EPT + e] = mk<T>(0, 0);
+            if (!valid) v[e] = v[EPT + e] = mk<T>(0, 0);
+            else if constexpr (YS::TMA) YS::load(tile, y, v[e], v[EPT + e]);
+            else ld2<T>(col + 2 * y, v[e], v[EPT + e]);
         }
         __syncthreads();   // the staging buffer is free: fetch the next column group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
@@ -735,6 +952,10 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
         }
     }
     cp_async_wait<0>();
+    if constexpr (YS::TMA) {
+        if (lost && threadIdx.x == 0) mbar_wait(&bar, phase, nullptr);   // bounded drain
+    }
+    (void)lost;
     (void)en;
 }
 

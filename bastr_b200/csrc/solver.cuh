@@ -29,6 +29,9 @@ struct Geo {
     // a NaN'`), and every kernel launched after it in the batch returns without touching data, so
     // the state stays the one that produced the NaN.
     unsigned int* halt;
+    // Error word of the handle (never null in a handle's launches): kernels record failures
+    // there (e.g. a TMA completion wait that gave up), and the host reports them after the batch.
+    unsigned int* err;
 };
 
 // True when an earlier kernel of the batch found a NaN energy; the same for every thread of the

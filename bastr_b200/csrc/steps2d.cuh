@@ -41,8 +41,14 @@ cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const 
         const double b = MODE == XM_RHS ? mix * 6 * cs : MODE == XM_RHS_VG ? mix * 8 * cs
                        : MODE == XM_TO_PHYS ? mix * 2 * cs + phys : phys + mix * 2 * cs;
         ProfScope ps(h, MODE == XM_RHS_VG ? "k2d_xpass_vg" : MODE == XM_RHS ? "k2d_xpass" : "k2d_xpass_state", b);
+        // the x maps describe the compute precision's records: only that precision's product
+        // modes are TMA-staged
+        if (P::TMA && sizeof(T) != (h->fp32 ? 4u : 8u)) return cudaErrorInvalidValue;
+        // tensor maps of the TMA-staged modes: the MA records of ftot fields (and the q pieces)
+        const CUtensorMap& ta = h->tm[ftot == 8 ? TM_XA8 : TM_XA4];
+        const CUtensorMap& tb = h->tm[TM_XB8];
         LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MA, ftot, (cplx<T>*)MB, pin, pout, vg, h->g,
-                                                twp<T>(h->tw[0])));
+                        twp<T>(h->tw[0]), ta, tb));
     });
     return cudaGetLastError();
 }
@@ -59,7 +65,8 @@ cudaError_t l2_yfwd(bastr_handle* h, const void* MB, StageIO<T> io, int from_u0)
         const double cs = sizeof(cplx<T>);
         ProfScope ps(h, "k2d_yfwd", (double)h->g.K * h->g.ny * 2 * cs +
                                     epi_bytes(EPI, from_u0, (double)h->g.K * h->g.KY * 2, cs));
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1])));
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]),
+                        h->tm[sizeof(T) == 8 ? TM_YMB64 : TM_YMB32]));
     });
     return cudaGetLastError();
 }
@@ -77,7 +84,7 @@ cudaError_t l2_yfwd_inv(bastr_handle* h, const void* MB, StageIO<T> io, int from
                                         epi_bytes(EPI, from_u0, (double)h->g.K * h->g.KY * 2, cs) +
                                         (double)h->g.ny * h->g.K * 4 * cs);
         LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, io, from_u0, h->g, twp<T>(h->tw[1]),
-                        (cplx<T>*)MA));
+                        (cplx<T>*)MA, h->tm[sizeof(T) == 8 ? TM_YMB64 : TM_YMB32]));
     });
     return cudaGetLastError();
 }
