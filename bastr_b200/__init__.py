@@ -44,7 +44,10 @@ EXPORTED = [
     "bastr_ensemble_tune", "bastr_ensemble_last_error",
     "bastr_net_nparams", "bastr_net_grad_blocks", "bastr_net_forward", "bastr_net_grad", "bastr_net_adam",
     "bastr_closure_apply", "bastr_transfer", "bastr_hitgen",
+    "bastr_h5_write", "bastr_h5_read", "bastr_h5_write_field", "bastr_h5_read_field", "bastr_h5_last_error",
 ]
+BASTR_H5_F64 = 0
+BASTR_H5_I32 = 1
 BASTR_E_TOO_LARGE = -6
 
 
@@ -71,6 +74,11 @@ class CStepOut(C.Structure):
         ("velgrad", C.c_double * 8), ("factor", C.c_double), ("E", C.c_double),
         ("energy", C.c_double), ("Fen", C.c_double),
     ]
+
+
+class CH5Dataset(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("type", C.c_int32), ("rank", C.c_int32), ("dims", C.c_int64 * 4),
+                ("data", C.c_void_p)]
 
 
 class CKernelStat(C.Structure):
@@ -127,6 +135,13 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_closure_apply.argtypes = [P, P, C.c_float, C.c_double]
     lib.bastr_transfer.argtypes = [P, D, D, D]
     lib.bastr_hitgen.argtypes = [P, C.c_int32, C.c_uint64, D, D, D, D, D]
+    lib.bastr_h5_write.argtypes = [C.c_char_p, C.POINTER(CH5Dataset), C.c_int32]
+    lib.bastr_h5_read.argtypes = [C.c_char_p, C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                  P, C.c_int64]
+    lib.bastr_h5_write_field.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, D, D, D, C.c_int64, C.c_double]
+    lib.bastr_h5_read_field.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, D, D, D,
+                                        C.POINTER(C.c_int64), D]
+    lib.bastr_h5_last_error.argtypes = [C.c_char_p, C.c_int32]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -335,6 +350,79 @@ class BastrGPU:
         self._check(self.lib.bastr_fft(self.h, a.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
                                        direction))
         return a
+
+
+# -------------------------------------------------------------------------------------------
+# Field files without libhdf5 (the HDF5 subset of hdf5io.F90's field files; host code only)
+# -------------------------------------------------------------------------------------------
+def _h5_check(lib, rc: int):
+    if rc != BASTR_OK:
+        buf = C.create_string_buffer(512)
+        lib.bastr_h5_last_error(buf, 512)
+        raise BastrError(rc, buf.value.decode(errors="replace"))
+
+
+def h5_write(path: str, datasets: dict):
+    """Writes {name: array} (float64 or int32 arrays, C order) as the root-group datasets of an
+    HDF5 file (bastr_h5_write)."""
+    lib = load_library()
+    keep, sets = [], []
+    for name, a in datasets.items():
+        a = np.ascontiguousarray(a)
+        if a.dtype == np.float64:
+            t = BASTR_H5_F64
+        elif a.dtype == np.int32:
+            t = BASTR_H5_I32
+        else:
+            raise ValueError(f"{name}: only float64 and int32 datasets")
+        if a.ndim == 0:
+            a = a.reshape(1)
+        dims = (C.c_int64 * 4)(*(list(a.shape) + [0] * (4 - a.ndim)))
+        keep.append(a)
+        sets.append(CH5Dataset(name.encode(), t, a.ndim, dims, a.ctypes.data))
+    arr = (CH5Dataset * max(len(sets), 1))(*sets)
+    _h5_check(lib, lib.bastr_h5_write(path.encode(), arr, len(sets)))
+
+
+def h5_read(path: str, name: str, dtype=np.float64) -> np.ndarray:
+    """One dataset of an HDF5 field file (bastr_h5_read), as a C-order array."""
+    lib = load_library()
+    t = BASTR_H5_I32 if np.dtype(dtype) == np.int32 else BASTR_H5_F64
+    rank = C.c_int32()
+    dims = (C.c_int64 * 4)()
+    _h5_check(lib, lib.bastr_h5_read(path.encode(), name.encode(), t, C.byref(rank), dims, None, 0))
+    out = np.empty([dims[i] for i in range(rank.value)], dtype=np.int32 if t == BASTR_H5_I32 else np.float64)
+    _h5_check(lib, lib.bastr_h5_read(path.encode(), name.encode(), t, C.byref(rank), dims,
+                                     C.c_void_p(out.ctypes.data), out.nbytes))
+    return out
+
+
+def write_field(path: str, u, nstep: int | None = None, time: float = 0.0):
+    """The reference's field file (writeflfed, readwrite.F90:222-257): u = [u1, u2(, u3)] arrays of
+    shape (ja, ia) or (ka, ja, ia), x fastest; nstep and time are written when nstep is given."""
+    lib = load_library()
+    arrs = [np.ascontiguousarray(c, dtype=np.float64) for c in u]
+    if arrs[0].ndim == 2:
+        ka, (ja, ia) = 0, arrs[0].shape
+    else:
+        ka, ja, ia = arrs[0].shape
+    u3 = arrs[2] if ka else arrs[0]
+    _h5_check(lib, lib.bastr_h5_write_field(path.encode(), ia, ja, ka, _dptr(arrs[0]), _dptr(arrs[1]), _dptr(u3),
+                                            -1 if nstep is None else int(nstep), float(time)))
+
+
+def read_field(path: str, ia: int, ja: int, ka: int = 0, counters: bool = False):
+    """u1, u2(, u3) of a field file on an ia x ja (x ka) grid (read_initial_field /
+    read_continue_field, readwrite.F90:114-220); with counters, also (nstep, time)."""
+    lib = load_library()
+    shape = (ja, ia) if ka == 0 else (ka, ja, ia)
+    out = [np.empty(shape) for _ in range(2 if ka == 0 else 3)]
+    n, t = C.c_int64(), C.c_double()
+    u3 = out[2] if ka else out[0]
+    _h5_check(lib, lib.bastr_h5_read_field(path.encode(), ia, ja, ka, _dptr(out[0]), _dptr(out[1]), _dptr(u3),
+                                           C.byref(n) if counters else None,
+                                           C.byref(t) if counters else None))
+    return (out, n.value, t.value) if counters else out
 
 
 from .ensemble import BastrEnsemble, ensemble_configs, partition_by_cost  # noqa: E402,F401

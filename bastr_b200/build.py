@@ -31,6 +31,7 @@ UNITS = {
     "steps3d_f32.cu": _COMMON + ["pass2d.cu", "pass3d.cu", "steps3d.cuh"],
     "steps3d_f64.cu": _COMMON + ["pass2d.cu", "pass3d.cu", "steps3d.cuh"],
     "noalloc.cu": ["solver.cuh", "fft_engine.cuh"],
+    "h5field.cpp": [],
 }
 # every source file of the library (for callers that check staleness as a whole)
 DEPS = sorted({d for u, ds in UNITS.items() for d in ds + [u]})
@@ -39,7 +40,7 @@ FLAGS = ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", 
 
 
 def _obj(unit: str) -> str:
-    return os.path.join(OBJDIR, unit[:-3] + ".o")
+    return os.path.join(OBJDIR, os.path.splitext(unit)[0] + ".o")
 
 
 def _mtime(p: str) -> float:

@@ -71,6 +71,9 @@ template <typename T> struct EptOf { static constexpr int v = sizeof(T) == 8 ? B
 #ifndef BASTR_EPT_XPASS_F32
 #define BASTR_EPT_XPASS_F32 16
 #endif
+#ifndef BASTR_XPASS_ZA
+#define BASTR_XPASS_ZA 3
+#endif
 // Blocks per SM asked of the register allocator: two once an FP32 block has 256 threads.
 template <typename T, int NT> constexpr int minb_for() { return sizeof(T) == 4 && NT >= 256 ? 2 : BASTR_MINB_2D; }
 template <int N, int EPT> constexpr int ept_fit() { return N < EPT ? N : EPT; }
@@ -258,8 +261,8 @@ template <typename T, int NX, int MODE> struct XPass2D {
     static constexpr int FIN = MODE == XM_RHS ? 4 : MODE == XM_RHS_VG ? 8 : MODE == XM_TO_PHYS ? 2 : 0;
     static constexpr int FLIVE = MODE == XM_RHS_VG ? 6 : FIN;
     static constexpr int EPT = ept_fit<NX, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_XPASS_F32>();
-    // at most three units share one shared-memory exchange; more run as a second transform
-    static constexpr int ZA = ZU > 3 ? 3 : ZU, ZB = ZU - ZA;
+    // at most BASTR_XPASS_ZA units share one shared-memory exchange; more run as a second transform
+    static constexpr int ZA = ZU > BASTR_XPASS_ZA ? BASTR_XPASS_ZA : ZU, ZB = ZU - ZA;
     using IFFT = RegFFT<T, NX, EPT, ZA, true>;
     using IFFTB = RegFFT<T, NX, EPT, (ZB > 0 ? ZB : 1), true>;
     using FFFT = RegFFT<T, NX, EPT, 1, false>;

@@ -184,6 +184,48 @@ BASTR_API int bastr_spectra_noalloc(int32_t ia, int32_t ja, int32_t ka, int32_t 
 /* Copies the message of the last failed call into buf (NUL-terminated); returns its length. */
 BASTR_API int bastr_last_error(bastr_handle* h, char* buf, int32_t n);
 
+/* ------------------------------------------------------------------------------------------
+ * Field files without libhdf5: the subset of HDF5 the reference's field files use, read and
+ * written from the HDF5 file format specification (host code only; no GPU, no handle).
+ * Replaces, for a caller without libhdf5, hdf5io.F90's h5io_init/h5write/h5read/h5srite/h5io_end
+ * as readwrite.F90 uses them: writeflfed (readwrite.F90:222-257; hdf5io.F90:752-802 h5wa3d_r8_struct,
+ * 1009-1184 h5_write1int/h5_write1rl8), read_initial_field / read_continue_field
+ * (readwrite.F90:114-220; hdf5io.F90:204-256 h5ra3d_r8_struct, 404-452 h5r_int4/h5r_real8).
+ * Files: HDF5 superblock version 0, root group as a symbol table, datasets of IEEE little-endian
+ * binary64 (H5T_NATIVE_DOUBLE) or signed 32-bit integers (H5T_NATIVE_INTEGER) with contiguous
+ * storage, the format libhdf5 writes by default; the reader also takes version 1 superblocks,
+ * object-header continuation blocks and compact storage.  Dimensions are in C order (slowest
+ * first), the reverse of Fortran's.
+ *
+ *   bastr_h5_write        a file holding the n datasets in its root group (replaced if it exists)
+ *   bastr_h5_read         one dataset: its rank and dims (dims[4], C order), and its values into
+ *                         data when data is not NULL (capacity in bytes; BASTR_E_INVALID if short)
+ *   bastr_h5_write_field  the reference's field file: u1, u2[, u3] as (ia+1, ja+1, ka+1) Fortran
+ *                         arrays holding the grid values in [0:ia, 0:ja, 0:max(ka,1)) and zero in
+ *                         the padding, plus nstep (int32) and time when nstep >= 0; u* host arrays
+ *                         x fastest, as bastr_set_state takes them
+ *   bastr_h5_read_field   the grid values of u1, u2[, u3] and, when the pointers are not NULL,
+ *                         nstep and time (flowini files have no counters: pass NULL)
+ *   bastr_h5_last_error   message of the calling thread's last failed bastr_h5_* call
+ * ------------------------------------------------------------------------------------------ */
+#define BASTR_H5_F64 0
+#define BASTR_H5_I32 1
+typedef struct bastr_h5_dataset {
+    const char* name;
+    int32_t type;                /* BASTR_H5_F64 or BASTR_H5_I32 */
+    int32_t rank;                /* 1..4 */
+    int64_t dims[4];             /* C order, slowest first */
+    const void* data;
+} bastr_h5_dataset;
+BASTR_API int bastr_h5_write(const char* path, const bastr_h5_dataset* sets, int32_t n);
+BASTR_API int bastr_h5_read(const char* path, const char* name, int32_t type, int32_t* rank, int64_t* dims,
+                            void* data, int64_t capacity);
+BASTR_API int bastr_h5_write_field(const char* path, int32_t ia, int32_t ja, int32_t ka, const double* u1,
+                                   const double* u2, const double* u3, int64_t nstep, double time);
+BASTR_API int bastr_h5_read_field(const char* path, int32_t ia, int32_t ja, int32_t ka, double* u1, double* u2,
+                                  double* u3, int64_t* nstep, double* time);
+BASTR_API int bastr_h5_last_error(char* buf, int32_t n);
+
 
 /* ------------------------------------------------------------------------------------------
  * Plan of a handle: its persistent grids use 1/2^share_log2 of the blocks that fit on the GPU

@@ -52,7 +52,7 @@ module bastr_gpu_mod
 
   public :: bastr_create, bastr_destroy, bastr_set_state, bastr_get_state, bastr_set_counters, &
             bastr_get_counters, bastr_step, bastr_spectra, bastr_fft, bastr_transfer, bastr_hitgen, &
-            bastr_last_error, bastr_error_message
+            bastr_h5_write_field, bastr_h5_read_field, bastr_last_error, bastr_error_message
 
   interface
     integer(c_int) function bastr_create(p, h) bind(c, name='bastr_create')
@@ -133,6 +133,29 @@ module bastr_gpu_mod
       integer(c_int32_t), value :: variant
       integer(c_int64_t), value :: seed
       real(c_double), intent(out) :: u1(*), u2(*), u3(*), angle(*), stats(8)
+    end function
+
+    ! field files without libhdf5 (the HDF5 subset of hdf5io.F90's files): writeflfed's
+    ! u1,u2[,u3] + nstep/time (nstep < 0: no counters, as in flowini files), and the reads of
+    ! read_initial_field / read_continue_field (pass c_null_ptr-backed optionals as needed)
+    integer(c_int) function bastr_h5_write_field(path, ia, ja, ka, u1, u2, u3, nstep, time) &
+        bind(c, name='bastr_h5_write_field')
+      import :: c_int, c_char, c_int32_t, c_int64_t, c_double
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t), value :: ia, ja, ka
+      real(c_double), intent(in) :: u1(*), u2(*), u3(*)
+      integer(c_int64_t), value :: nstep
+      real(c_double), value :: time
+    end function
+
+    integer(c_int) function bastr_h5_read_field(path, ia, ja, ka, u1, u2, u3, nstep, time) &
+        bind(c, name='bastr_h5_read_field')
+      import :: c_int, c_char, c_int32_t, c_int64_t, c_double
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t), value :: ia, ja, ka
+      real(c_double), intent(out) :: u1(*), u2(*), u3(*)
+      integer(c_int64_t), intent(out) :: nstep
+      real(c_double), intent(out) :: time
     end function
 
     integer(c_int) function bastr_last_error(h, buf, n) bind(c, name='bastr_last_error')
