@@ -45,6 +45,7 @@ EXPORTED = [
     "bastr_net_nparams", "bastr_net_grad_blocks", "bastr_net_forward", "bastr_net_grad", "bastr_net_adam",
     "bastr_closure_apply", "bastr_transfer", "bastr_hitgen",
     "bastr_h5_write", "bastr_h5_read", "bastr_h5_write_field", "bastr_h5_read_field", "bastr_h5_last_error",
+    "bastr_subgrid", "bastr_ensemble_subgrid", "bastr_ensemble_run",
 ]
 BASTR_H5_F64 = 0
 BASTR_H5_I32 = 1
@@ -142,6 +143,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_h5_read_field.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, D, D, D,
                                         C.POINTER(C.c_int64), D]
     lib.bastr_h5_last_error.argtypes = [C.c_char_p, C.c_int32]
+    lib.bastr_subgrid.argtypes = [P, C.c_int32, P, P]
+    lib.bastr_ensemble_subgrid.argtypes = [P, C.c_int32, C.c_int32, P, P]
+    lib.bastr_ensemble_run.argtypes = [P, C.c_int32, C.c_int32, D]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -314,6 +318,16 @@ class BastrGPU:
                                           _dptr(u3) if u3 is not None else None, _dptr(angle), _dptr(st)))
         names = ("energy", "factor", "alpha", "residual", "QX", "QY", "QZ", "QW")
         return out, angle, dict(zip(names, st.tolist()))
+
+    def subgrid(self, r: int):
+        """(ub, tau) of the current state as float32 CUDA tensors [d][...coarse grid] (bastr_subgrid):
+        the box-filtered velocity and the subgrid term filter(u.grad u) - ub.grad ub."""
+        import torch
+        shape = [self.ndims] + [n // r for n in self.shape]
+        ub = torch.empty(shape, dtype=torch.float32, device="cuda")
+        tau = torch.empty_like(ub)
+        self._check(self.lib.bastr_subgrid(self.h, r, C.c_void_p(ub.data_ptr()), C.c_void_p(tau.data_ptr())))
+        return ub, tau
 
     def closure_apply(self, net, scale: float, dt: float):
         """One closure sub-step u <- u - dt * scale * net(u) on this (3D) solver's state; `net` is

@@ -5,9 +5,10 @@ without the closure, per spectrum shell, with the GPU time of each run.
                                        [--spinup 400] [--every 100] [--snapshots 4] [--steps 400]
                                        [--iters 2000] [--out FILE]
 
-1. Training data: fine runs (linear forcing, FP32 form) from seeded fields; after `--spinup`
-   steps, every `--every` steps the velocity and its advective term are box-filtered onto the
-   coarse grid: pairs (ub, tau = filter(u.grad u) - ub.grad ub).
+1. Training data from the batched solver: one fine realization per training seed (linear forcing,
+   FP32 form) in one ensemble, advanced by CUDA-graph replays; after `--spinup` steps, every
+   `--every` steps each realization's filtered field and subgrid term are formed on the device
+   (bastr_ensemble_subgrid): pairs (ub, tau = filter(u.grad u) - ub.grad ub).
 2. The network is trained on those pairs (tau scaled by its RMS) by the library's kernels.
 3. Test: a fine run from the held-out seed; at the end of its spin-up its filtered field starts
    two coarse runs (same dt), one plain and one with the closure sub-step after every step.
@@ -20,52 +21,71 @@ from __future__ import annotations
 
 import argparse
 import json
-import time
 
 import numpy as np
 
 
-def _sync_time(fn):
+def _device_ms(stream, fn):
+    """Device time in ms of the work fn() enqueues on `stream` (CUDA events on that stream)."""
     import torch
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream.synchronize()
+    e0.record(stream)
     out = fn()
-    torch.cuda.synchronize()
-    return out, time.perf_counter() - t0
+    e1.record(stream)
+    stream.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def _advance(s, n):
+    """n steps on a handle without reading records back (chunks of at most 256)."""
+    while n > 0:
+        c = min(n, 256)
+        s.step_async(c)
+        n -= c
 
 
 def run(args) -> dict:
     import torch
-    from . import BastrGPU, seeded_field
-    from .closure import Net, box_filter, filtered_pair
+    from . import BastrEnsemble, BastrGPU, seeded_field
+    from .closure import Net
 
     nf, r = args.fine, args.ratio
     nc = nf // r
     phys = dict(reynolds=args.reynolds, deltat=args.dt, forcemethod=1, target_energy=args.target)
+    batch = args.batch
+    if args.spinup % batch or args.every % batch:
+        raise ValueError("spinup and every must be multiples of batch")
+    stream = torch.cuda.Stream()
 
     def fine_solver():
-        return BastrGPU(nf, nf, nf, precision="fp32", velgrad_every=0, kmax=nf // 3, **phys)
+        s = BastrGPU(nf, nf, nf, precision="fp32", velgrad_every=0, kmax=nf // 3, **phys)
+        s.set_stream(stream.cuda_stream)
+        return s
 
-    def dev(a):
-        return torch.tensor(np.ascontiguousarray(a, np.float32), device="cuda")
-
-    # 1. training pairs
+    # 1. training pairs, made by the batched solver: one fine realization per training seed, advanced
+    #    together by CUDA-graph replays; at every snapshot each realization's filtered field and
+    #    subgrid term are formed on the device (bastr_ensemble_subgrid)
+    cfgs = [dict(ia=nf, ja=nf, ka=nf, precision="fp32", velgrad_every=0, kmax=nf // 3, seed=sd, **phys)
+            for sd in args.train_seeds]
     pairs = []
-    for seed in args.train_seeds:
-        with fine_solver() as s:
-            s.set_state(seeded_field(nf, nf, nf, k0=args.k0, seed=seed))
-            s.step(args.spinup)
-            for _ in range(args.snapshots):
-                s.step(args.every)
-                pairs.append(filtered_pair(s, s.get_state(), r))
-    tau_rms = float(np.sqrt(np.mean(np.stack([t for _, t in pairs]) ** 2)))
-    train = [(dev(ub), dev(t / tau_rms)) for ub, t in pairs]
+    dns_ms = 0.0
+    with BastrEnsemble(cfgs) as ens:
+        for i, sd in enumerate(args.train_seeds):
+            ens.set_state(i, seeded_field(nf, nf, nf, k0=args.k0, seed=sd))
+        dns_ms += ens.run(args.spinup, batch)
+        for _ in range(args.snapshots):
+            dns_ms += ens.run(args.every, batch)
+            pairs += [ens.subgrid(i, r) for i in range(len(cfgs))]
+    tau_rms = float(torch.sqrt(torch.mean(torch.stack([t for _, t in pairs]) ** 2)).item())
+    train = [(ub.contiguous(), (t / tau_rms).contiguous()) for ub, t in pairs]
 
-    # 2. training
+    # 2. training, by the library's forward / backward / Adam kernels
     net = Net(seed=args.net_seed)
-    hist, t_train = _sync_time(lambda: net.train(train, iters=args.iters, lr=args.lr))
+    cur = torch.cuda.current_stream()
+    hist, t_train = _device_ms(cur, lambda: net.train(train, iters=args.iters, lr=args.lr))
 
-    # 3. test
+    # 3. test: the held-out fine run (the judge), and two coarse runs from its filtered field
     def coarse_spectrum(fields):
         with BastrGPU(nc, nc, nc, **phys) as c:
             c.set_state(fields)
@@ -74,15 +94,15 @@ def run(args) -> dict:
 
     with fine_solver() as s:
         s.set_state(seeded_field(nf, nf, nf, k0=args.k0, seed=args.test_seed))
-        s.step(args.spinup)
-        ub0 = [box_filter(c, r) for c in s.get_state()]
-        _, t_fine = _sync_time(lambda: s.step(args.steps))
-        u1 = s.get_state()
-        ub1, tau1 = filtered_pair(s, u1, r)   # held-out pair for the a-priori error
-    e_dns = coarse_spectrum([box_filter(c, r) for c in u1])
+        _advance(s, args.spinup)
+        ub0 = [c for c in s.subgrid(r)[0].cpu().numpy().astype(np.float64)]
+        _, t_fine = _device_ms(stream, lambda: _advance(s, args.steps))
+        ub1, tau1 = (x.cpu().numpy() for x in s.subgrid(r))   # held-out pair for the a-priori error
+    e_dns = coarse_spectrum([c.astype(np.float64) for c in ub1])
 
     def coarse_run(closure: bool):
         with BastrGPU(nc, nc, nc, precision="fp32", velgrad_every=0, **phys) as c:
+            c.set_stream(stream.cuda_stream)
             c.set_state(ub0)
 
             def go():   # no host round trip per step: records are not read back
@@ -91,8 +111,7 @@ def run(args) -> dict:
                     if closure and (i + 1) % args.closure_every == 0:
                         # one split sub-step covering the last closure_every steps
                         c.closure_apply(net, tau_rms, args.dt * args.closure_every)
-                c.sync()
-            _, t = _sync_time(go)
+            _, t = _device_ms(stream, go)
             return coarse_spectrum(c.get_state()), t
 
     e_plain, t_plain = coarse_run(False)
@@ -104,19 +123,19 @@ def run(args) -> dict:
         return {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()),
                 "shells_within_5pct": int((rel <= 0.05).sum()), "shells": int(rel.size)}
 
-    pred = net.forward(dev(ub1), scale=tau_rms).cpu().numpy()
+    pred = net.forward(torch.tensor(ub1, device="cuda"), scale=tau_rms).cpu().numpy()
     apriori = {"mse_closure": float(np.mean((pred - tau1) ** 2)), "mse_no_closure": float(np.mean(tau1 ** 2))}
     return {
         "fine": nf, "coarse": nc, "filter_width_cells": r, "reynolds": args.reynolds, "dt": args.dt,
         "train_seeds": args.train_seeds, "test_seed": args.test_seed, "pairs": len(pairs),
         "spinup_steps": args.spinup, "test_steps": args.steps, "iters": args.iters, "tau_rms": tau_rms,
-        "closure_every": args.closure_every,
-        "loss_first": hist[0], "loss_last": hist[-1], "train_gpu_s": t_train,
-        "fine_gpu_s": t_fine, "coarse_plain_gpu_s": t_plain, "coarse_closure_gpu_s": t_clos,
+        "closure_every": args.closure_every, "training_data": "batched solver (bastr_ensemble_run + bastr_ensemble_subgrid)",
+        "loss_first": hist[0], "loss_last": hist[-1], "train_gpu_ms": t_train, "training_dns_gpu_ms": dns_ms,
+        "fine_gpu_ms": t_fine, "coarse_plain_gpu_ms": t_plain, "coarse_closure_gpu_ms": t_clos,
         "speedup_closure_vs_fine": t_fine / t_clos,
         "E_dns": e_dns[1:kc].tolist(), "E_plain": e_plain[1:kc].tolist(), "E_closure": e_clos[1:kc].tolist(),
         "error_plain": err(e_plain), "error_closure": err(e_clos), "apriori_held_out": apriori,
-        "timing": "host wall time with device synchronisation around each run; coarse runs launch asynchronously",
+        "timing": "device time: CUDA events on the stream the runs launch on",
     }
 
 
@@ -137,6 +156,7 @@ def main():
     ap.add_argument("--iters", type=int, default=2000)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--net-seed", type=int, default=0)
+    ap.add_argument("--batch", type=int, default=10, help="steps per CUDA-graph replay of the training ensemble")
     ap.add_argument("--closure-every", type=int, default=1,
                     help="apply the closure once every this many coarse steps (sub-step dt times it)")
     ap.add_argument("--out", default=None)

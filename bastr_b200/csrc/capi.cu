@@ -7,20 +7,22 @@
 #include "closure.cu"
 #include "transfer.cu"
 #include "hitgen.cu"
+#include "subgrid.cu"
 
 using namespace bastr_impl;
 
 namespace {
 
 // One axis of the full-grid transform on the device array A (complex, [nz][ny][nx]).
-template <bool INV> cudaError_t full_axis(bastr_handle* h, double2* A, int axis, double scale) {
-    const Geo& g = h->g;
-    const int ns[3] = {g.nx, g.ny, g.nz};
-    const long long total = (long long)g.nx * g.ny * g.nz;
+// One axis of the full-grid transform of a complex grid A of extents ns[3] ([nz][ny][nx]) with
+// the twiddle table tw of that axis's length.
+template <bool INV>
+cudaError_t full_axis_n(bastr_handle* h, double2* A, const int ns[3], int axis, double scale, const double2* tw) {
+    const long long total = (long long)ns[0] * ns[1] * ns[2];
     const int N = ns[axis];
     const int nlines = (int)(total / N);
-    const long long S = axis == 0 ? 1 : axis == 1 ? g.nx : (long long)g.nx * g.ny;
-    const long long R = axis == 1 ? (long long)g.nx * g.ny : g.nx;
+    const long long S = axis == 0 ? 1 : axis == 1 ? ns[0] : (long long)ns[0] * ns[1];
+    const long long R = axis == 1 ? (long long)ns[0] * ns[1] : ns[0];
     SIZE_CASES(N, {
         using P = FullLine<NN>;
         auto k = k_full_axis<NN, INV>;
@@ -28,9 +30,15 @@ template <bool INV> cudaError_t full_axis(bastr_handle* h, double2* A, int axis,
         cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(nlines, P::G), &grid);
         if (e != cudaSuccess) return e;
         ProfScope ps(h, "k_full_axis", (double)total * 32);
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, A, g.nx, S, R, nlines, scale, (const double2*)h->tw[axis].d64));
+        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, A, ns[0], S, R, nlines, scale, tw));
     });
     return cudaGetLastError();
+}
+
+// One axis of the full-grid transform on the handle's own grid.
+template <bool INV> cudaError_t full_axis(bastr_handle* h, double2* A, int axis, double scale) {
+    const int ns[3] = {h->g.nx, h->g.ny, h->g.nz};
+    return full_axis_n<INV>(h, A, ns, axis, scale, (const double2*)h->tw[axis].d64);
 }
 
 // bastr_fft: host array -> the handle's physical-field buffer (2 or 3 doubles per point, so a
@@ -216,6 +224,7 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
 
 void free_all(bastr_handle* h) {
     void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->rng, h->closure_buf, h->tr_buf, h->tr_modes, h->hg_part,
+                    h->sg_buf, h->sg_tw,
                     h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
                     h->sp_item_part};
     for (void* q : ptrs)
@@ -928,6 +937,92 @@ int bastr_hitgen(bastr_handle* h, int32_t variant, uint64_t seed, double* u1, do
         const double v[8] = {energy, factor, bis ? alpha : std::nan(""), check, q[0], q[1], q[2], q[3]};
         for (int i = 0; i < 8; ++i) stats[i] = v[i];
     }
+    return BASTR_OK;
+}
+
+// Filtered fields and the subgrid term of the current state (subgrid.cu), for closure training:
+// d_ubar, d_tau: device arrays of d * (nx/r)(ny/r)(nz/r) floats, [component][coarse grid], x
+// fastest (either may be NULL).  Work buffers are allocated on the first call (and when r changes).
+int bastr_subgrid(bastr_handle* h, int32_t r, float* d_ubar, float* d_tau) {
+    if (!h) return BASTR_E_INVALID;
+    if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
+    const Geo& g = h->g;
+    const int D = g.d;
+    if (r < 2 || (r & (r - 1)) || g.nx % r || g.ny % r || (D == 3 && g.nz % r))
+        return fail(h, BASTR_E_INVALID, "filter width %d must be a power of two dividing the grid", r);
+    const int cns[3] = {g.nx / r, g.ny / r, D == 3 ? g.nz / r : 1};
+    for (int a = 0; a < D; ++a)
+        if (cns[a] < 16) return fail(h, BASTR_E_UNSUPPORTED, "coarse extents below 16 are not built");
+    if (!d_ubar && !d_tau) return fail(h, BASTR_E_INVALID, "no output");
+    CK(cudaSetDevice(h->device));
+    const size_t N = (size_t)g.nx * g.ny * g.nz, nc = (size_t)cns[0] * cns[1] * cns[2];
+    if (h->sg_r != r) {
+        if (h->sg_buf) CK(cudaFree(h->sg_buf));
+        if (h->sg_tw) CK(cudaFree(h->sg_tw));
+        h->sg_buf = nullptr;
+        h->sg_tw = nullptr;
+        h->sg_r = 0;
+        CK(cudaMalloc(&h->sg_buf, (3 * N + nc * (4 * (size_t)D + 3)) * sizeof(double)));
+        CK(cudaMalloc(&h->sg_tw, (size_t)(cns[0] + cns[1] + cns[2]) * sizeof(double2)));
+        size_t o = 0;
+        for (int a = 0; a < 3; ++a) {
+            std::vector<double2> t64;
+            std::vector<float2> t32;
+            host_twiddles(cns[a], t64, t32);
+            CK(cudaMemcpy(h->sg_tw + o, t64.data(), cns[a] * sizeof(double2), cudaMemcpyHostToDevice));
+            o += cns[a];
+        }
+        h->sg_r = r;
+    }
+    const double2* ctw[3] = {h->sg_tw, h->sg_tw + cns[0], h->sg_tw + cns[0] + cns[1]};
+    double2* W = reinterpret_cast<double2*>(h->sg_buf);          // fine complex scratch
+    double* acc = h->sg_buf + 2 * N;                               // fine products
+    double* ub = acc + N;                                          // [D][nc]
+    double* fadv = ub + D * nc;                                    // [D][nc]
+    double* cadv = fadv + D * nc;                                  // [nc]
+    double2* uh = reinterpret_cast<double2*>(cadv + nc);           // [D][nc] spectra of ub
+    double2* Wc = uh + D * nc;                                     // coarse complex scratch
+    cudaStream_t st = h->stream;
+    const int gs = 148 * 8;
+    CK(flush_pending_scale(h));
+    CK(to_physical(h));                                            // h->phys = u, [D][N]
+    // filter(u_j d_j u_i) on the fine grid
+    for (int i = 0; i < D; ++i) {
+        for (int j = 0; j < D; ++j) {
+            CK(cudaMemsetAsync(W, 0, N * sizeof(double2), st));
+            if (D == 2) k_sg_scatter<2><<<gs, 256, 0, st>>>(h->u0, g, i, j, W);
+            else k_sg_scatter<3><<<gs, 256, 0, st>>>(h->u0, g, i, j, W);
+            CK(cudaGetLastError());
+            for (int a = 0; a < D; ++a) CK(full_axis<true>(h, W, a, 1.0));
+            k_sg_accum<<<gs, 256, 0, st>>>(acc, h->phys + (size_t)j * N, W, N, j == 0);
+            CK(cudaGetLastError());
+        }
+        k_sg_filter<<<gs, 256, 0, st>>>(acc, g.nx, g.ny, g.nz, r, D, fadv + (size_t)i * nc);
+        CK(cudaGetLastError());
+    }
+    // ub and its spectra on the coarse grid
+    for (int c = 0; c < D; ++c) {
+        k_sg_filter<<<gs, 256, 0, st>>>(h->phys + (size_t)c * N, g.nx, g.ny, g.nz, r, D, ub + (size_t)c * nc);
+        k_sg_complex<<<gs, 256, 0, st>>>(ub + (size_t)c * nc, uh + (size_t)c * nc, nc);
+        CK(cudaGetLastError());
+        for (int a = 0; a < D; ++a)
+            CK(full_axis_n<false>(h, uh + (size_t)c * nc, cns, a, a == D - 1 ? 1.0 / (double)nc : 1.0, ctw[a]));
+    }
+    // ub_j d_j ub_i on the coarse grid, and the outputs
+    for (int i = 0; i < D; ++i) {
+        for (int j = 0; j < D; ++j) {
+            k_sg_deriv<<<gs, 256, 0, st>>>(uh + (size_t)i * nc, Wc, cns[0], cns[1], cns[2], j);
+            CK(cudaGetLastError());
+            for (int a = 0; a < D; ++a) CK(full_axis_n<true>(h, Wc, cns, a, 1.0, ctw[a]));
+            k_sg_accum<<<gs, 256, 0, st>>>(cadv, ub + (size_t)j * nc, Wc, nc, j == 0);
+            CK(cudaGetLastError());
+        }
+        k_sg_finish<<<gs, 256, 0, st>>>(fadv + (size_t)i * nc, cadv, ub + (size_t)i * nc,
+                                         d_tau ? d_tau + (size_t)i * nc : nullptr,
+                                         d_ubar ? d_ubar + (size_t)i * nc : nullptr, nc);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(st));
     return BASTR_OK;
 }
 

@@ -218,6 +218,58 @@ int bastr_ensemble_step(bastr_ensemble* e, int32_t nsteps, bastr_step_out* out) 
     return status;
 }
 
+// Advances the ensemble by nsteps = k * batch steps as k replays of the batch graph, timed on the
+// device with events on the ensemble's stream around all of them; only the last batch's records
+// stay (bastr_ensemble_step reads them for a batch).  device_ms: total device time.
+int bastr_ensemble_run(bastr_ensemble* e, int32_t nsteps, int32_t batch, double* device_ms) {
+    if (!e || batch < 1 || batch > kChunk || nsteps < 0 || nsteps % batch)
+        return efail(e, BASTR_E_INVALID, "nsteps must be a multiple of batch, batch in [1, %d]", kChunk);
+    for (size_t i = 0; i < e->hs.size(); ++i)
+        if (!e->hs[i]->have_state) return efail(e, BASTR_E_STATE, "realization %zu: no state set", i);
+    ECK(cudaSetDevice(e->device));
+    if (e->exec_steps != batch || !e->exec) {
+        const int r = capture(e, batch);
+        if (r) return r;
+    }
+    cudaEvent_t a = nullptr, b = nullptr;
+    ECK(cudaEventCreate(&a));
+    ECK(cudaEventCreate(&b));
+    const int k = nsteps / batch;
+    cudaError_t st = cudaEventRecord(a, e->main);
+    for (int i = 0; i < k && st == cudaSuccess; ++i) st = cudaGraphLaunch(e->exec, e->main);
+    if (st == cudaSuccess) st = cudaEventRecord(b, e->main);
+    if (st == cudaSuccess) st = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (st == cudaSuccess) st = cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (st != cudaSuccess) return efail(e, BASTR_E_CUDA, "ensemble run: %s", cudaGetErrorString(st));
+    if (device_ms) *device_ms = ms;
+    // host bookkeeping: the first k-1 batches advance the counters, the last one also reads the
+    // stop words (a realization that stopped keeps stopping at once in every later batch)
+    for (int i = 0; i + 1 < k; ++i)
+        for (bastr_handle* h : e->hs)
+            for (int j = 0; j < batch; ++j) {
+                h->nstep += 1;
+                h->time = h->time + h->p.deltat;
+            }
+    if (k > 0) after_batch(e, batch);
+    for (size_t i = 0; i < e->hs.size(); ++i)
+        if (k > 0 && e->host_halt[i] != 0)
+            return efail(e, BASTR_E_NAN, "realization %zu: \"E\" is a NaN at nstep %lld", i,
+                         (long long)e->hs[i]->nstep);
+    return BASTR_OK;
+}
+
+// Filtered fields and subgrid term of realization i's current state (bastr_subgrid): the
+// ensemble's output as closure training data.
+int bastr_ensemble_subgrid(bastr_ensemble* e, int32_t i, int32_t r, float* d_ubar, float* d_tau) {
+    if (!e || i < 0 || i >= (int)e->hs.size()) return efail(e, BASTR_E_INVALID, "realization index");
+    const int rc = bastr_subgrid(e->hs[i], r, d_ubar, d_tau);
+    if (rc) e->err = "realization " + std::to_string(i) + ": " + e->hs[i]->err;
+    return rc;
+}
+
 // Sets the plan of realization i (-1: all) and drops the captured graph.
 int bastr_ensemble_set_plan(bastr_ensemble* e, int32_t i, int32_t share_log2) {
     if (!e) return BASTR_E_INVALID;

@@ -83,6 +83,9 @@ struct bastr_handle {
     double2* tr_buf = nullptr;     // transfer spectra: full complex grids (allocated on first use)
     double* tr_modes = nullptr;    // transfer spectra: per-mode values, item partials, shell sums
     double* hg_part = nullptr;     // initial-field generators: per-block partial sums
+    double* sg_buf = nullptr;      // filtered fields / subgrid term: work buffers (allocated on first use)
+    double2* sg_tw = nullptr;      // ... and the coarse grid's twiddle tables
+    int sg_r = 0;                  // filter width the work buffers were sized for
     double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
     unsigned long long* rng = nullptr;  // forcing calls so far: counter of the random-phase stream
     bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra

@@ -134,6 +134,24 @@ class BastrEnsemble:
             raise self._BastrError(rc, self._err())
         return recs
 
+    def run(self, nsteps: int, batch: int = 10) -> float:
+        """Advances every realization by nsteps (a multiple of batch) as replays of the batch graph;
+        returns the device time in ms (events on the ensemble's stream around all replays)."""
+        ms = C.c_double()
+        self._check(self.lib.bastr_ensemble_run(self.e, nsteps, batch, C.byref(ms)))
+        return ms.value
+
+    def subgrid(self, i: int, r: int):
+        """(ub, tau) of realization i's current state as float32 CUDA tensors (bastr_ensemble_subgrid):
+        the batched solver's closure training data."""
+        import torch
+        shape = [self.ndims[i]] + [n // r for n in self.shapes[i]]
+        ub = torch.empty(shape, dtype=torch.float32, device="cuda")
+        tau = torch.empty_like(ub)
+        self._check(self.lib.bastr_ensemble_subgrid(self.e, i, r, C.c_void_p(ub.data_ptr()),
+                                                    C.c_void_p(tau.data_ptr())))
+        return ub, tau
+
     def set_plan(self, share_log2: int, i: int = -1):
         self._check(self.lib.bastr_ensemble_set_plan(self.e, i, share_log2))
 

@@ -300,16 +300,20 @@ def fp32_accuracy(device, steps={"2d2048": 100, "3d256": 20}):
     return out
 
 
-def ensemble_measure(device, steps=30, tune=True):
+def ensemble_measure(device, steps=1000, batch=10, seq_steps=100, peak=None, tune=True):
     """The standard ensemble (96 realizations: 32 each at 256^2, 512^2, 1024^2, seeds 0-95, band
-    forcing with forcek in {3..8}, target in [0.05, 0.1], FP32), advanced as one CUDA graph per
-    batch of steps; host wall time around the synchronous ensemble step calls (records read
-    back every batch), and the same realizations stepped one after another through their own
-    handles for comparison."""
+    forcing with forcek in {3..8}, target in [0.05, 0.1], FP32), advanced `steps` steps as replays of
+    one CUDA graph per batch of `batch` steps, device-timed (events on the ensemble's stream around
+    all replays, BastrEnsemble.run).  Beside it: the same realizations stepped one after another
+    through their own handles (device-timed per realization over `seq_steps` steps), and the device
+    time of the closure training data (filtered field and subgrid term, r = 4) of one 1024^2
+    realization.  B_model of an ensemble step: the sum of the realizations' 66 V (2D)."""
+    import torch
     from bastr_b200 import BastrEnsemble, BastrGPU, ensemble_configs, seeded_field
     cfgs = ensemble_configs()
     fields = [seeded_field(c["ia"], c["ja"], 0, k0=c["k0"], seed=c["seed"]) for c in cfgs]
-    out = {"realizations": len(cfgs), "sizes": sorted({c["ia"] for c in cfgs}), "precision": "fp32"}
+    out = {"realizations": len(cfgs), "sizes": sorted({c["ia"] for c in cfgs}), "precision": "fp32",
+           "steps": steps, "batch": batch}
     with BastrEnsemble(cfgs, device=device) as ens:
         for i, u in enumerate(fields):
             ens.set_state(i, u)
@@ -317,27 +321,42 @@ def ensemble_measure(device, steps=30, tune=True):
             out["tuned_ms_per_step"] = round(ens.tune(nsteps=4, reps=2, max_share_log2=3), 4)
             out["plans_log2_by_size"] = {str(n): sorted({p for c, p in zip(cfgs, ens.plans()) if c["ia"] == n})
                                          for n in out["sizes"]}
-        batch = 10
-        ens.step(batch)   # capture of the batch graph + warm-up
-        t0 = time.perf_counter()
-        for _ in range(steps // batch):
-            ens.step(batch)
-        dt = time.perf_counter() - t0
-        steps = (steps // batch) * batch
-    out["ensemble_steps_per_s"] = round(steps / dt, 2)
-    out["realization_steps_per_s"] = round(steps * len(cfgs) / dt, 1)
-    # one realization after another, each through its own handle
+            for i, u in enumerate(fields):
+                ens.set_state(i, u)
+        ens.run(3 * batch, batch)        # capture of the batch graph + warm-up
+        ms = ens.run(steps, batch)
+        i1024 = next(i for i, c in enumerate(cfgs) if c["ia"] == 1024)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ens.subgrid(i1024, 4)            # allocates the work buffers
+        torch.cuda.synchronize()
+        e0.record()
+        ens.subgrid(i1024, 4)
+        e1.record()
+        torch.cuda.synchronize()
+        out["subgrid_ms_1024"] = round(e0.elapsed_time(e1), 3)
+    t_step = ms / steps
+    out["device_ms_per_step"] = round(t_step, 4)
+    out["ensemble_steps_per_s"] = round(1e3 / t_step, 2)
+    out["realization_steps_per_s"] = round(len(cfgs) * 1e3 / t_step, 1)
+    b_model = sum(66 * c["ia"] * c["ja"] * 4 for c in cfgs)
+    out["b_model_bytes_per_step"] = b_model
+    if peak:
+        out["survey_roofline_frac"] = round(b_model / (t_step * 1e-3) / (peak * 1e9), 4)
+    # one realization after another, each through its own handle, device-timed
     t_seq = 0.0
     for c, u in zip(cfgs, fields):
         with BastrGPU(c["ia"], c["ja"], 0, deltat=c["deltat"], forcemethod=2, forcek=c["forcek"],
                       target_energy=c["target_energy"], lprojectd=True, precision="fp32", device=device) as s:
             s.set_state(u)
-            s.step(2)
-            t1 = time.perf_counter()
-            s.step(steps)
-            t_seq += time.perf_counter() - t1
-    out["sequential_realization_steps_per_s"] = round(steps * len(cfgs) / t_seq, 1)
-    out["timing"] = "host wall time around synchronous step calls (records copied to the host each call)"
+            stream = torch.cuda.Stream(device=device)
+            s.set_stream(stream.cuda_stream)
+            run_steps(s, 3)
+            s.sync()
+            t_seq += device_time(s, stream, seq_steps) / seq_steps
+    out["sequential_ms_per_step"] = round(t_seq, 4)
+    out["sequential_realization_steps_per_s"] = round(len(cfgs) * 1e3 / t_seq, 1)
+    out["timing"] = "CUDA events on the launching streams (device time), inputs resident"
     return out
 
 
@@ -477,8 +496,8 @@ def ours(args):
     # the same end-to-end measure in the FP64 form, the reference's own precision
     e2e64 = (e2e_measure(wl, "fp64", max(20, min(args.steps, 200)), device)
              if (rank == 0 and not args.no_e2e and prec != "fp64") else None)
-    ens = (ensemble_measure(device) if (rank == 0 and n_gpus == 1 and not args.no_variants and not args.no_ensemble)
-           else None)
+    ens = (ensemble_measure(device, peak=peak) if (rank == 0 and n_gpus == 1 and not args.no_variants
+                                                  and not args.no_ensemble) else None)
     base = cpu_baseline(wl) if (rank == 0 and n_gpus == 1 and not args.no_cpu) else None
     acc = fp32_accuracy(device) if (rank == 0 and n_gpus == 1 and not args.no_variants) else None
     if dist_ctx:

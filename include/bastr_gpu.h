@@ -259,6 +259,9 @@ BASTR_API int bastr_ensemble_get_plan(bastr_ensemble* e, int32_t* share_log2);
 BASTR_API int bastr_ensemble_tune(bastr_ensemble* e, int32_t nsteps, int32_t reps, int32_t max_share_log2,
                                   double* best_ms);
 BASTR_API int bastr_ensemble_last_error(bastr_ensemble* e, char* buf, int32_t n);
+/* nsteps = k * batch steps as k replays of the batch graph, device time (events on the ensemble's
+ * stream around all k) in *device_ms; the records of the last batch are kept. */
+BASTR_API int bastr_ensemble_run(bastr_ensemble* e, int32_t nsteps, int32_t batch, double* device_ms);
 
 /* ------------------------------------------------------------------------------------------
  * Learned subgrid closure for a coarse 3D solve (no reference counterpart).  A local network
@@ -284,6 +287,17 @@ BASTR_API int bastr_net_grad(int32_t nx, int32_t ny, int32_t nz, const float* d_
 BASTR_API int bastr_net_adam(float* d_w, uint16_t* d_wb, float* d_m, float* d_v, const float* d_g, int32_t t,
                              float lr, float b1, float b2, float eps, void* stream);
 BASTR_API int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float scale, double dt);
+
+/* Closure training data from a handle's current state, on the device (no reference counterpart):
+ * the box filter of width r (mean over r^d cells, decimation r) of the velocity, ub, and the
+ * subgrid term tau_i = filter(u_j d_j u_i) - ub_j d_j ub_i, spectral derivatives on the fine and
+ * the coarse grid, FP64 arithmetic.  d_ubar, d_tau (either may be NULL): device arrays of
+ * d * (ia/r)(ja/r)(ka/r) floats, [component][coarse grid], x fastest.  r is a power of two that
+ * divides every extent, leaving coarse extents of at least 16.  Allocates its work buffers (three
+ * fine real grids' worth) on the first call.  bastr_ensemble_subgrid does the same for
+ * realization i of an ensemble: the batched solver's output as the closure's training data. */
+BASTR_API int bastr_subgrid(bastr_handle* h, int32_t r, float* d_ubar, float* d_tau);
+BASTR_API int bastr_ensemble_subgrid(bastr_ensemble* e, int32_t i, int32_t r, float* d_ubar, float* d_tau);
 
 #ifdef __cplusplus
 }

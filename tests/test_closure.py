@@ -137,3 +137,21 @@ def test_trained_closure_beats_no_closure_on_filtered_dns(gpu_lib):
     mse_none = float(np.mean(tau ** 2))
     assert mse_net < 0.7 * mse_none, (mse_net, mse_none)
     torch.cuda.synchronize()
+
+
+def test_closure_study_runs_from_ensemble_data(gpu_lib):
+    """The a-posteriori study end to end at a small size: training pairs from the batched solver
+    (bastr_ensemble_subgrid), training by the library's kernels, the held-out filtered DNS against
+    the plain and the closure coarse runs, device-timed."""
+    import argparse
+
+    from bastr_b200.closure_study import run
+    args = argparse.Namespace(fine=64, ratio=4, reynolds=40.0, dt=1e-3, target=1.5, k0=3.0, train_seeds=[0, 1],
+                              test_seed=7, spinup=20, every=10, snapshots=2, steps=20, iters=60, lr=2e-3,
+                              net_seed=0, batch=10, closure_every=1)
+    res = run(args)
+    assert res["pairs"] == 4 and res["training_data"].startswith("batched solver")
+    assert res["loss_last"] < res["loss_first"]
+    assert res["apriori_held_out"]["mse_closure"] < res["apriori_held_out"]["mse_no_closure"]
+    assert res["fine_gpu_ms"] > 0 and res["coarse_closure_gpu_ms"] > 0
+    assert len(res["E_dns"]) == len(res["E_closure"]) > 0
