@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HEADER = os.path.join(ROOT, "include", "bastr_gpu.h")
 
-_COMMON = ["handle.cuh", "solver.cuh", "fft_engine.cuh", "regfft.cuh", "tma.cuh"]
+_COMMON = ["handle.cuh", "solver.cuh", "fft_engine.cuh", "regfft.cuh", "tma.cuh", "umma.cuh"]
 # translation unit -> the sources it includes
 UNITS = {
     "capi.cu": _COMMON + ["diag.cu", "fullfft.cu", "closure.cu", "transfer.cu", "hitgen.cu", "subgrid.cu",

@@ -771,9 +771,9 @@ int bastr_net_forward(int32_t nx, int32_t ny, int32_t nz, const float* d_u, cons
                       float scale, void* stream) {
     if (nx < 3 || ny < 3 || nz < 3 || !d_u || !d_w || !d_out) return BASTR_E_INVALID;
     const size_t n = (size_t)nx * ny * nz;
-    const int grid = (int)std::min<size_t>((n + 127) / 128, 148 * 8);
-    k_net_forward<float><<<grid, 128, 0, (cudaStream_t)stream>>>(d_u, (const __nv_bfloat16*)d_w, d_out, nx, ny, nz,
-                                                                  scale);
+    const int grid = (int)std::min<size_t>((n + kFwdNT - 1) / kFwdNT, 148 * 4);
+    k_net_forward_tc<float><<<grid, kFwdNT, kFwdSmem, (cudaStream_t)stream>>>(d_u, (const __nv_bfloat16*)d_w, d_out,
+                                                                            nx, ny, nz, scale, nullptr);
     return cudaGetLastError() == cudaSuccess ? BASTR_OK : BASTR_E_CUDA;
 }
 
@@ -1037,9 +1037,10 @@ int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float scale, doubl
     if (!h->closure_buf) CK(cudaMalloc(&h->closure_buf, 3 * n * sizeof(float)));
     CK(flush_pending_scale(h));
     CK(to_physical(h));
-    const int grid = (int)std::min<size_t>((n + 127) / 128, 148 * 8);
-    k_net_forward<double><<<grid, 128, 0, h->stream>>>(h->phys, (const __nv_bfloat16*)d_w, h->closure_buf, h->g.nx,
-                                                        h->g.ny, h->g.nz, scale);
+    const int grid = (int)std::min<size_t>((n + kFwdNT - 1) / kFwdNT, 148 * 4);
+    k_net_forward_tc<double><<<grid, kFwdNT, kFwdSmem, h->stream>>>(h->phys, (const __nv_bfloat16*)d_w,
+                                                                      h->closure_buf, h->g.nx, h->g.ny, h->g.nz,
+                                                                      scale, h->done + T_ERR);
     CK(cudaGetLastError());
     k_closure_update<<<148 * 4, 256, 0, h->stream>>>(h->phys, h->closure_buf, 3 * n, dt);
     CK(cudaGetLastError());

@@ -4,9 +4,13 @@ checker of the CUDA network kernels; nothing in the product calls it).
 The network and its parameter layout are the ones the CUDA kernels implement
 (bastr_b200/csrc/closure.cu): layer 1 a periodic 3x3x3 stencil 3 -> 32 channels, layers 2 and 3
 pointwise 32 -> 32, layer 4 pointwise 32 -> 3, GELU (tanh form) after layers 1-3.  Weights are
-used as BF16 (round to nearest even of the FP32 master value); everything else here is FP64.
-The loss is mean((net(u) - tau)^2) over points and channels; the gradient is back-propagation
-written out by hand, and `fd_gradient` differentiates the loss numerically to check it.
+used as BF16 (round to nearest even of the FP32 master value), and so are the inputs of every
+layer (the taps and the activations h1..h3, rounded FP64 -> FP32 -> BF16 as the kernels round
+their FP32 values) unless ``act_bf16=False``; the products and sums are FP64.  The loss is
+mean((net(u) - tau)^2) over points and channels; the gradient is back-propagation written out by
+hand, passing the rounding of layer inputs through unchanged (its derivative taken as 1, as the
+kernels do), and `fd_gradient` differentiates the smooth loss (``act_bf16=False``) numerically
+to check it.
 There is no reference counterpart: the closure extends the reference's solver.
 """
 from __future__ import annotations
@@ -73,13 +77,20 @@ def taps(u: np.ndarray) -> np.ndarray:
     return np.stack(cols, axis=1).astype(np.float64)
 
 
-def forward(u: np.ndarray, w: np.ndarray, keep: bool = False):
-    """net(u) [3][nz][ny][nx] with BF16-rounded weights."""
+def _act(h: np.ndarray, act_bf16: bool) -> np.ndarray:
+    return bf16_round(h.astype(np.float32)).astype(np.float64) if act_bf16 else h
+
+
+def forward(u: np.ndarray, w: np.ndarray, keep: bool = False, act_bf16: bool = True):
+    """net(u) [3][nz][ny][nx] with BF16-rounded weights (and layer inputs, with act_bf16)."""
     W1, b1, W2, b2, W3, b3, W4, b4 = unpack(bf16_round(w))
-    x = taps(u)
+    x = _act(taps(u), act_bf16)
     h1, d1 = gelu(x @ W1.T + b1)
+    h1 = _act(h1, act_bf16)
     h2, d2 = gelu(h1 @ W2.T + b2)
+    h2 = _act(h2, act_bf16)
     h3, d3 = gelu(h2 @ W3.T + b3)
+    h3 = _act(h3, act_bf16)
     out = h3 @ W4.T + b4
     res = out.T.reshape((3,) + u.shape[1:])
     if keep:
@@ -87,10 +98,10 @@ def forward(u: np.ndarray, w: np.ndarray, keep: bool = False):
     return res
 
 
-def loss_grad(u: np.ndarray, tau: np.ndarray, w: np.ndarray):
+def loss_grad(u: np.ndarray, tau: np.ndarray, w: np.ndarray, act_bf16: bool = True):
     """loss = mean((net(u) - tau)^2) and d loss / d w (with respect to the BF16-rounded weights)."""
     W1, b1, W2, b2, W3, b3, W4, b4 = unpack(bf16_round(w))
-    _, (x, h1, d1, h2, d2, h3, d3, out) = forward(u, w, keep=True)
+    _, (x, h1, d1, h2, d2, h3, d3, out) = forward(u, w, keep=True, act_bf16=act_bf16)
     t = np.stack([tau[c].ravel() for c in range(3)], axis=1).astype(np.float64)
     r = out - t
     n = r.shape[0]

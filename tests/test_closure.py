@@ -35,7 +35,42 @@ def test_forward_matches_oracle(gpu_lib):
     w = _weights(2)
     net = Net(weights=w)
     got = net.forward(_tensor(u), scale=1.5).cpu().numpy()
-    assert _rel(got, 1.5 * co.forward(u.astype(np.float64), w)) < 1e-5
+    # tensor-core forward: BF16 layer inputs, FP32 sums.  The oracle rounds the same inputs from
+    # its FP64 values, so an input whose FP32 and FP64 values straddle a BF16 rounding boundary
+    # rounds differently (about 6e-5 relative L2 in an FP32 simulation): tolerance 5e-4.
+    assert _rel(got, 1.5 * co.forward(u.astype(np.float64), w)) < 5e-4
+
+
+def test_forward_tiles_and_extents(gpu_lib):
+    """Point counts that are not a multiple of the 128-point tile, extents of 3 (every neighbour
+    wraps), many tiles per block, and two calls in a row give the same bits."""
+    from bastr_b200.closure import Net
+    from oracle import closure_oracle as co
+    rng = np.random.default_rng(11)
+    w = _weights(12)
+    net = Net(weights=w)
+    for shape in [(3, 3, 3, 3), (3, 5, 7, 9), (3, 24, 40, 36)]:
+        u = rng.standard_normal(shape).astype(np.float32)
+        got = net.forward(_tensor(u)).cpu().numpy()
+        assert np.all(np.isfinite(got))
+        assert _rel(got, co.forward(u.astype(np.float64), w)) < 5e-4, shape
+        again = net.forward(_tensor(u)).cpu().numpy()
+        assert np.array_equal(got, again)
+
+
+def test_forward_and_training_loss_agree(gpu_lib):
+    """The tensor-core forward (inference) and the training kernel's forward use the same
+    arithmetic: the loss of one equals the loss of the other up to FP32 summation order."""
+    import torch
+    from bastr_b200.closure import Net
+    rng = np.random.default_rng(13)
+    u = rng.standard_normal((3, 16, 16, 16)).astype(np.float32)
+    tau = rng.standard_normal((3, 16, 16, 16)).astype(np.float32)
+    net = Net(weights=_weights(14))
+    loss, _ = net.loss_grad(_tensor(u), _tensor(tau))
+    pred = net.forward(_tensor(u))
+    l2 = float(torch.mean((pred.double() - _tensor(tau).double()) ** 2))
+    assert abs(loss - l2) / l2 < 1e-5
 
 
 def test_bf16_copy_matches_oracle_rounding(gpu_lib):
@@ -56,8 +91,9 @@ def test_loss_and_gradient_match_oracle(gpu_lib):
     net = Net(weights=w)
     loss, g = net.loss_grad(_tensor(u), _tensor(tau))
     rl, rg = co.loss_grad(u.astype(np.float64), tau.astype(np.float64), w)
-    assert abs(loss - rl) / rl < 1e-5
-    assert _rel(g.cpu().numpy(), rg) < 1e-4
+    # BF16 layer inputs rounded from FP32 here and from FP64 in the oracle (see the forward test)
+    assert abs(loss - rl) / rl < 1e-4
+    assert _rel(g.cpu().numpy(), rg) < 1e-3
     # deterministic: the same call gives the same bits
     _, g2 = net.loss_grad(_tensor(u), _tensor(tau))
     assert np.array_equal(g.cpu().numpy(), g2.cpu().numpy())
@@ -110,7 +146,8 @@ def test_closure_apply_matches_host(gpu_lib):
     k1, k2, k3 = generate_wave(p)
     m = dealias_mask(p, np.sqrt(k1 * k1 + k2 * k2 + k3 * k3))
     want = np.stack([np.fft.ifftn(np.fft.fftn(u[c] - dt * scale * tau[c]) * m).real for c in range(3)])
-    assert _rel(got, want) < 1e-6
+    # the sub-step's change of the state, against the oracle's network (BF16 layer inputs: 5e-4)
+    assert _rel(got - u, want - u) < 5e-4
 
 
 def test_trained_closure_beats_no_closure_on_filtered_dns(gpu_lib):

@@ -32,7 +32,7 @@ def test_gradient_matches_finite_differences():
     w = co.init_weights(1)
     w[co.OFF_B1:co.OFF_W2] = rng.uniform(-0.1, 0.1, co.C)   # non-zero biases exercise those paths
     w[co.OFF_B4:co.NP] = rng.uniform(-0.1, 0.1, 3)
-    loss, g = co.loss_grad(u, tau, w)
+    loss, g = co.loss_grad(u, tau, w, act_bf16=False)
     assert loss > 0
     idx = [0, 7, 80, co.OFF_B1 + 3, co.OFF_W2 + 5, co.OFF_B2 + 1, co.OFF_W3 + 100, co.OFF_B3 + 31,
            co.OFF_W4 + 40, co.OFF_B4 + 2]
@@ -45,3 +45,13 @@ def test_adam_moves_against_gradient():
     g = np.array([1, -1, 0, 2, -3], np.float32)
     w1, m, v = co.adam(w, np.zeros(5, np.float32), np.zeros(5, np.float32), g, 1, 1e-2)
     assert np.all(np.sign(w - w1) == np.sign(g))
+
+
+def test_bf16_layer_inputs_change_little():
+    """Rounding every layer's input to BF16 moves the output by about the BF16 resolution."""
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal((3, 4, 5, 6))
+    w = co.init_weights(2)
+    a, b = co.forward(u, w, act_bf16=True), co.forward(u, w, act_bf16=False)
+    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert 1e-5 < rel < 2 ** -6
