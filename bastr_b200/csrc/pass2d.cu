@@ -263,6 +263,8 @@ template <typename T, int NX, int MODE> struct XPass2D {
     static constexpr int EPT = ept_fit<NX, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_XPASS_F32>();
     // at most BASTR_XPASS_ZA units share one shared-memory exchange; more run as a second transform
     static constexpr int ZA = ZU > BASTR_XPASS_ZA ? BASTR_XPASS_ZA : ZU, ZB = ZU - ZA;
+    // the second transform runs through the exchange buffer sized for the first
+    static_assert(ZB <= ZA, "BASTR_XPASS_ZA: the remaining units must fit the exchange of the first transform");
     using IFFT = RegFFT<T, NX, EPT, ZA, true>;
     using IFFTB = RegFFT<T, NX, EPT, (ZB > 0 ? ZB : 1), true>;
     using FFFT = RegFFT<T, NX, EPT, 1, false>;
