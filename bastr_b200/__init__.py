@@ -256,8 +256,14 @@ class BastrGPU:
         u3 = arrs[2] if self.ndims == 3 else arrs[0]
         self._check(self.lib.bastr_set_state(self.h, _dptr(arrs[0]), _dptr(arrs[1]), _dptr(u3)))
 
-    def get_state(self):
-        out = [np.empty(self.shape, dtype=np.float64) for _ in range(self.ndims)]
+    def get_state(self, out=None):
+        """The physical velocity components; into `out` (one C-contiguous float64 array of the
+        grid's shape per component, e.g. pinned host memory) when given."""
+        if out is None:
+            out = [np.empty(self.shape, dtype=np.float64) for _ in range(self.ndims)]
+        elif len(out) != self.ndims or any(o.shape != self.shape or o.dtype != np.float64 or
+                                           not o.flags.c_contiguous for o in out):
+            raise ValueError("get_state(out=...): one C-contiguous float64 array of the grid's shape per component")
         u3 = out[2] if self.ndims == 3 else out[0]
         self._check(self.lib.bastr_get_state(self.h, _dptr(out[0]), _dptr(out[1]), _dptr(u3)))
         return out

@@ -66,17 +66,21 @@ def run(args) -> dict:
     # 1. training pairs, made by the batched solver: one fine realization per training seed, advanced
     #    together by CUDA-graph replays; at every snapshot each realization's filtered field and
     #    subgrid term are formed on the device (bastr_ensemble_subgrid)
-    cfgs = [dict(ia=nf, ja=nf, ka=nf, precision="fp32", velgrad_every=0, kmax=nf // 3, seed=sd, **phys)
-            for sd in args.train_seeds]
+    #    (in ensembles of at most --group realizations, one after another, to bound device memory)
     pairs = []
     dns_ms = 0.0
-    with BastrEnsemble(cfgs) as ens:
-        for i, sd in enumerate(args.train_seeds):
-            ens.set_state(i, seeded_field(nf, nf, nf, k0=args.k0, seed=sd))
-        dns_ms += ens.run(args.spinup, batch)
-        for _ in range(args.snapshots):
-            dns_ms += ens.run(args.every, batch)
-            pairs += [ens.subgrid(i, r) for i in range(len(cfgs))]
+    group = args.group if args.group > 0 else len(args.train_seeds)
+    for g0 in range(0, len(args.train_seeds), group):
+        seeds = args.train_seeds[g0:g0 + group]
+        cfgs = [dict(ia=nf, ja=nf, ka=nf, precision="fp32", velgrad_every=0, kmax=nf // 3, seed=sd, **phys)
+                for sd in seeds]
+        with BastrEnsemble(cfgs) as ens:
+            for i, sd in enumerate(seeds):
+                ens.set_state(i, seeded_field(nf, nf, nf, k0=args.k0, seed=sd))
+            dns_ms += ens.run(args.spinup, batch)
+            for _ in range(args.snapshots):
+                dns_ms += ens.run(args.every, batch)
+                pairs += [ens.subgrid(i, r) for i in range(len(cfgs))]
     tau_rms = float(torch.sqrt(torch.mean(torch.stack([t for _, t in pairs]) ** 2)).item())
     train = [(ub.contiguous(), (t / tau_rms).contiguous()) for ub, t in pairs]
 
@@ -157,6 +161,8 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--net-seed", type=int, default=0)
     ap.add_argument("--batch", type=int, default=10, help="steps per CUDA-graph replay of the training ensemble")
+    ap.add_argument("--group", type=int, default=0,
+                    help="training realizations per ensemble (0: all in one); groups run one after another")
     ap.add_argument("--closure-every", type=int, default=1,
                     help="apply the closure once every this many coarse steps (sub-step dt times it)")
     ap.add_argument("--out", default=None)

@@ -367,6 +367,19 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
                         encode_map(&h->tm[TM_YMB32], h->mb, 4, 3, dy, sy32, by, 0) &&
                         encode_map(&h->tm[TM_YMB64], h->mb, 8, 3, dy, sy64, by, 64);
         if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a mixed-field tensor map");
+    } else if (cs == sizeof(float2) && K <= 256) {
+        // TMA tensor maps of MB [z][kx][f][y] for the FP32 3D x pass (see TensorMapSlot3): FP32
+        // values, 4 consecutive y (32 bytes) x every field x every kx x 1 z plane, 32-byte swizzle
+        const uint64_t NY = g.ny, KK = K, NZ = g.nz;
+        bool ok = true;
+        const int fins[2] = {9, 13};
+        for (int m = 0; m < 2; ++m) {
+            const uint64_t F = fins[m];
+            const uint64_t dm[4] = {2 * NY, F, KK, NZ}, sm[3] = {NY * 8, F * NY * 8, KK * F * NY * 8};
+            const uint32_t bx[4] = {8, (uint32_t)F, (uint32_t)KK, 1};
+            ok = ok && encode_map(&h->tm3[m], h->mb, 4, 4, dm, sm, bx, 32);
+        }
+        if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a 3D mixed-field tensor map");
     }
 
     const int ns[3] = {g.nx, g.ny, d == 3 ? g.nz : 0};
@@ -771,6 +784,7 @@ int bastr_net_forward(int32_t nx, int32_t ny, int32_t nz, const float* d_u, cons
                       float scale, void* stream) {
     if (nx < 3 || ny < 3 || nz < 3 || !d_u || !d_w || !d_out) return BASTR_E_INVALID;
     const size_t n = (size_t)nx * ny * nz;
+    if (3 * n >= ((size_t)1 << 31)) return BASTR_E_UNSUPPORTED;   // the kernel's 32-bit tap offsets
     const int grid = (int)std::min<size_t>((n + kFwdNT - 1) / kFwdNT, 148 * 4);
     k_net_forward_tc<float><<<grid, kFwdNT, kFwdSmem, (cudaStream_t)stream>>>(d_u, (const __nv_bfloat16*)d_w, d_out,
                                                                             nx, ny, nz, scale, nullptr);
@@ -1034,6 +1048,7 @@ int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float scale, doubl
     if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
     CK(cudaSetDevice(h->device));
     const size_t n = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    if (3 * n >= ((size_t)1 << 31)) return fail(h, BASTR_E_UNSUPPORTED, "closure network: grid too large");
     if (!h->closure_buf) CK(cudaMalloc(&h->closure_buf, 3 * n * sizeof(float)));
     CK(flush_pending_scale(h));
     CK(to_physical(h));

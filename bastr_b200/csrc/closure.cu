@@ -41,9 +41,11 @@ constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kNetC * kNetIn, kOffW2 = kOffB1 + kN
 // about 1e-6 relative error, far below the BF16 rounding of the result.  dg = d gelu / dz
 // = s + 2 z s (1 - s) sqrt(2/pi) (1 + 3 * 0.044715 z^2), s = sigmoid(2y).
 __device__ __forceinline__ float gelu_s(float z) {
-    const float a = 0.7978845608028654f, c = 0.044715f;
-    const float y = a * fmaf(c * z, z * z, z);
-    return __fdividef(z, 1.0f + __expf(-2.0f * y));
+    // e^-2y = 2^(z (k1 + k3 z^2)), k1 = -2 sqrt(2/pi) log2(e), k3 = 0.044715 k1
+    const float k1 = -2.302208198144325f, k3 = -0.10294324f;
+    float e;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(z * fmaf(k3, z * z, k1)));
+    return __fdividef(z, 1.0f + e);
 }
 __device__ __forceinline__ float gelu_t(float z, float& dg) {
     const float a = 0.7978845608028654f, c = 0.044715f;
@@ -236,16 +238,17 @@ __global__ void __launch_bounds__(kFwdNT, 4) k_net_forward_tc(const TI* __restri
         {
             const int x = valid ? (int)(p % nx) : 0, y = valid ? (int)((p / nx) % ny) : 0;
             const int z = valid ? (int)(p / ((size_t)nx * ny)) : 0;
+            // periodic neighbour offsets (n < 2^31 points: 32-bit offsets)
             const int xs[3] = {x == 0 ? nx - 1 : x - 1, x, x == nx - 1 ? 0 : x + 1};
-            const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
-            const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
+            const int yo[3] = {(y == 0 ? ny - 1 : y - 1) * nx, y * nx, (y == ny - 1 ? 0 : y + 1) * nx};
+            const int zo[3] = {(z == 0 ? nz - 1 : z - 1) * ny * nx, z * ny * nx, (z == nz - 1 ? 0 : z + 1) * ny * nx};
             float v[8];
 #pragma unroll
             for (int i = 0; i < kK1; ++i) {
                 float val = 0.0f;
                 if (i < kNetIn && valid) {
                     const int c = i / 27, dz = (i / 9) % 3, dy = (i / 3) % 3, dx = i % 3;
-                    val = (float)u[c * n + ((size_t)zs[dz] * ny + ys[dy]) * nx + xs[dx]];
+                    val = (float)u[(unsigned)(c * (int)n + zo[dz] + yo[dy] + xs[dx])];
                 }
                 v[i % 8] = val;
                 if (i % 8 == 7)

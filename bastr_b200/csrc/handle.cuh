@@ -118,6 +118,7 @@ struct bastr_handle {
     std::vector<int64_t> ecount;
     // TMA tensor maps of the mixed-field buffers (2D, compute precision), built at creation
     CUtensorMap tm[5] = {};
+    CUtensorMap tm3[2] = {};
 };
 
 namespace bastr_impl {
@@ -131,7 +132,11 @@ enum Ticket : int { T_SPECTRA = 0, T_HALT = 1, T_ERR = 2, kTickets = 4 };
 //   TM_XB8           the (q1, q2) pieces of the second record (ftot 8), box = 2 fields x 1 row x BK kx
 //   TM_YMB32/64      MB records [y/2][kx][2 rows][2 comps] in FP32 / FP64, box = 4 values x 1 kx x
 //                    BY row pairs (the FP64 one also serves the state transform of FP32 handles)
+// and of a 3D handle whose x pass stages with TMA (FP32, one warp's worth of threads per row):
+//   TM_X3MB9/13      MB [z][kx][f][y] of the product fields (9) / with the velocity-gradient
+//                    fields (13), FP32 values; box = 4 consecutive y x every f x every kx x 1 z
 enum TensorMapSlot : int { TM_XA4 = 0, TM_XA8 = 1, TM_XB8 = 2, TM_YMB32 = 3, TM_YMB64 = 4, kTensorMaps = 5 };
+enum TensorMapSlot3 : int { TM_X3MB9 = 0, TM_X3MB13 = 1 };
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point (no link to libcuda).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,

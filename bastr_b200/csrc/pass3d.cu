@@ -16,6 +16,7 @@
 //             (tool.F90:196-217), viscous term, projection (tool.F90:245-270), RK/CN combination.
 #include "regfft.cuh"
 #include "solver.cuh"
+#include "tma.cuh"
 
 namespace bastr {
 
@@ -259,11 +260,29 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
 // ---------------------------------------------------------------------------------------
 enum X3Mode : int { X3_RHS = 1, X3_RHS_VG = 2, X3_TO_PHYS = 3, X3_FROM_PHYS = 4 };
 
+// Units of the 3D x pass's inverse transforms that share one shared-memory exchange (the rest
+// run as further transforms through the same buffer), and the blocks per SM asked of the
+// register allocator for the FP32 product passes (0: no request).
+#ifndef BASTR_X3_ZA
+#define BASTR_X3_ZA 8
+#endif
+#ifndef BASTR_MINB_X3
+#define BASTR_MINB_X3 0
+#endif
+// Row pairing of the 3D x pass (0: one row per warp; 1: a row per half-warp; 2: rows alternating
+// every 8 lanes, the fastest at 256^3 FP32: 2.50 -> 2.47 ms per step).
+#ifndef BASTR_X3_PAIR
+#define BASTR_X3_PAIR 2
+#endif
+
 template <typename T, int NX, int MODE> struct XPass3D {
     static constexpr int FIN = MODE == X3_RHS ? 9 : MODE == X3_RHS_VG ? 13 : MODE == X3_TO_PHYS ? 3 : 0;
     static constexpr int ZU = MODE == X3_RHS ? 6 : MODE == X3_RHS_VG ? 8 : 2;
     static constexpr int EPT = ept_fit<NX, (MODE == X3_RHS || MODE == X3_RHS_VG) ? EptWide<T>::v : EptOf<T>::v>();
-    using IFFT = RegFFT<T, NX, EPT, ZU, true>;
+    static constexpr int ZA = ZU < BASTR_X3_ZA ? ZU : (BASTR_X3_ZA < 2 ? 2 : BASTR_X3_ZA);
+    using IFFT = RegFFT<T, NX, EPT, ZA, true>;
+    static constexpr int MINB = (BASTR_MINB_X3 > 0 && sizeof(T) == 4 && (MODE == X3_RHS || MODE == X3_RHS_VG))
+                                    ? BASTR_MINB_X3 : 1;
     using FFFT = RegFFT<T, NX, EPT, 2, false>;
     static constexpr int NTR = IFFT::NTR;
     // rows of one block: consecutive y of one z plane (every extent is a power of two >= 16)
@@ -277,19 +296,44 @@ template <typename T, int NX, int MODE> struct XPass3D {
     // tile unpadded, which leaves the velocity-gradient variant two blocks per SM)
     static constexpr int KPAD = (FIN * G * (int)sizeof(cplx<T>) / 16) % 2 == 0 ? 16 / (int)sizeof(cplx<T>) : 0;
     static constexpr int KSTR = FIN * G + KPAD;        // staged elements per kx
-    static constexpr int TSTR = sizeof(T) == 4 ? ((3 * G) | 1) : 3 * G;   // tile elements per kx
-    static constexpr size_t STAGE = MODE == X3_FROM_PHYS ? (size_t)G * 3 * NX * sizeof(double)
-                                                          : (size_t)KMAX * KSTR * sizeof(cplx<T>);
+    // rows served in pairs by pairs of warps (see k3d_xpass): with one warp's worth of threads
+    // per row, an even number of rows and exchange buffers a multiple of 128 bytes long
+    static constexpr bool PAIRED = BASTR_X3_PAIR > 0 && NTR == 32 && G % 2 == 0 &&
+                                   (IFFT::SMEM_ELEMS * (int)sizeof(cplx<T>)) % 128 == 0;
+    // tile elements per kx, odd in FP32 so that the split's stores of consecutive kx spread over
+    // the banks (an even stride that is conflict-free for paired rows measured slower: it pushed
+    // the velocity-gradient variant past its shared-memory budget)
+    static constexpr int TSTR = sizeof(T) == 4 ? ((3 * G) | 1) : 3 * G;
+    // TMA staging (the FP32 product passes with paired rows): the row group's [kx][f][4 rows]
+    // values as one box of a 4-D tensor map over MB, unpadded and swizzled at 32 bytes, which
+    // keeps the paired rows' 8-byte reads conflict-free; one elected thread issues it
+    static constexpr bool TMA = PAIRED && sizeof(T) == 4 && G == 4 && (MODE == X3_RHS || MODE == X3_RHS_VG) &&
+                                KMAX <= 256;
+    static constexpr uint32_t TX_BYTES = (uint32_t)(KMAX * FIN * G * sizeof(cplx<T>));
+    static constexpr size_t STAGE = TMA ? 1024 + (((size_t)TX_BYTES + 1023) & ~(size_t)1023)
+                                  : MODE == X3_FROM_PHYS ? (size_t)G * 3 * NX * sizeof(double)
+                                                         : (size_t)KMAX * KSTR * sizeof(cplx<T>);
     static constexpr size_t TILE = (size_t)KMAX * TSTR * sizeof(cplx<T>);   // output tile [kx][row][c]
     static constexpr size_t XCH = (size_t)G * IFFT::SMEM_ELEMS * sizeof(cplx<T>);
     static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
     static constexpr size_t SMEM = STAGE + TILE + XCHR;
 };
 
+// Inverse transforms of units [U0, ZU) in runs of at most ZA units through one exchange buffer.
+template <typename T, int NX, int EPT, int ZU, int ZA, int U0 = 0>
+__device__ __forceinline__ void x3_inverse_runs(cplx<T>* v, cplx<T>* sm, const cplx<T>* __restrict__ tw, int t) {
+    if constexpr (U0 < ZU) {
+        constexpr int NU = ZU - U0 < ZA ? ZU - U0 : ZA;
+        RegFFT<T, NX, EPT, NU, true>::run(v + U0 * EPT, sm, tw, t);
+        x3_inverse_runs<T, NX, EPT, ZU, ZA, U0 + NU>(v, sm, tw, t);
+    }
+}
+
 template <typename T, int NX, int MODE>
-__global__ void __launch_bounds__(XPass3D<T, NX, MODE>::NT)
+__global__ void __launch_bounds__(XPass3D<T, NX, MODE>::NT, XPass3D<T, NX, MODE>::MINB)
 k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double* __restrict__ phys_in,
-          double* __restrict__ phys_out, double* __restrict__ vg_part, Geo g, const cplx<T>* __restrict__ tw) {
+          double* __restrict__ phys_out, double* __restrict__ vg_part, Geo g, const cplx<T>* __restrict__ tw,
+          const __grid_constant__ CUtensorMap tmb) {
     pdl_wait();
     if (halted(g)) return;
     using P = XPass3D<T, NX, MODE>;
@@ -299,15 +343,46 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char* stg = smraw;
     cplx<T>* tile = reinterpret_cast<cplx<T>*>(smraw + P::STAGE);
-    const int gi = threadIdx.x / NTR, t = threadIdx.x % NTR;
+    // Row of this thread.  With one warp's worth of threads per row, the rows are taken in pairs
+    // by pairs of warps, alternating every 8 lanes (lanes with bit 3 clear serve row 2p + h, the
+    // others row 2p + 1 - h, for warp 2p + h; t = lane either way).  The two rows' staged values
+    // sit in opposite halves of each 16-byte chunk, so each half-warp's 8-byte loads of
+    // consecutive wavenumbers reach all 32 banks once (one row alone reaches only the banks of one
+    // half: 2-way conflicts).  The rows' exchange buffers are a multiple of 128 bytes apart, so the
+    // exchanges keep their bank pattern.
+    constexpr bool PAIRED = P::PAIRED;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int gi = !PAIRED ? threadIdx.x / NTR
+                 : BASTR_X3_PAIR == 1 ? 2 * (wp >> 1) + ((wp & 1) ^ (lane >> 4))
+                                      : 2 * (wp >> 1) + (((lane >> 3) & 1) ^ (wp & 1));
+    const int t = PAIRED ? lane : threadIdx.x % NTR;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::TILE) + gi * IFFT::SMEM_ELEMS;
     const int K = g.K, NY = g.ny;
     const int rows = NY * g.nz;
     const size_t npts = (size_t)NX * rows;
     const int nitems = (rows + G - 1) / G;
+    // TMA tile at the first 1024-byte boundary of the staging area
+    unsigned char* tmat = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    __shared__ __align__(8) uint64_t bar;
+    if constexpr (P::TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    uint32_t phase = 0;
+    bool lost = false;   // a TMA completion wait gave up (recorded in g.err)
     auto issue = [&](int item) {
         const int r0 = item * G;   // G consecutive y rows of one z plane
-        if constexpr (MODE == X3_FROM_PHYS) {
+        if constexpr (P::TMA) {
+            if (threadIdx.x == 0) {
+                const int z0 = r0 / NY, y0 = r0 - z0 * NY;
+                mbar_expect_tx(&bar, P::TX_BYTES);
+                tma_load_4d(tmat, &tmb, 2 * y0, 0, 0, z0, &bar);
+            }
+            return;
+        } else if constexpr (MODE == X3_FROM_PHYS) {
             double* d = reinterpret_cast<double*>(stg);
 #pragma unroll
             for (int c = 0; c < 3; ++c) stage_line(d + (size_t)c * G * NX, phys_in + c * npts + (size_t)r0 * NX, G * NX * 8);
@@ -336,8 +411,17 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
     int item = blockIdx.x;
     if (item < nitems) issue(item);
     for (; item < nitems; item += gridDim.x) {
-        cp_async_wait<0>();
-        __syncthreads();
+        if constexpr (P::TMA) {
+            const bool ok = mbar_wait(&bar, phase, g.err);
+            if (__syncthreads_or(!ok)) {   // block-uniform: stop, and drain below
+                lost = true;
+                break;
+            }
+            phase ^= 1u;
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         const int row = item * G + gi;   // row = z*NY + y
         const bool valid = row < rows;
         cplx<T> v[ZU * EPT];
@@ -363,7 +447,12 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
                 if (IFFT::in_band(e, NX / 3 + 1)) continue;
                 if (valid && (lo || hi)) {
                     const cplx<T>* src0 = rw + (size_t)k * P::KSTR;
-                    auto src = [&](int f) { return src0[f * G]; };
+                    auto src = [&](int f) -> cplx<T> {
+                        if constexpr (P::TMA)
+                            return *reinterpret_cast<const cplx<T>*>(
+                                tmat + swz<32>((uint32_t)((k * FIN + f) * G + gi) * (uint32_t)sizeof(cplx<T>)));
+                        else return src0[f * G];
+                    };
                     const bool z0 = p == 0;
                     if constexpr (MODE == X3_TO_PHYS) {
                         v[e] = pack_at<T>(src(0), src(1), hi, z0);
@@ -393,7 +482,7 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
         }
         __syncthreads();   // the staging buffer is free: fetch the next row group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
-        if constexpr (MODE != X3_FROM_PHYS) IFFT::run(v, sm, tw, t);
+        if constexpr (MODE != X3_FROM_PHYS) x3_inverse_runs<T, NX, EPT, ZU, P::ZA>(v, sm, tw, t);
 
         if constexpr (MODE == X3_TO_PHYS) {
             if (valid) {
@@ -475,6 +564,10 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
         }
     }
     cp_async_wait<0>();
+    if constexpr (P::TMA) {
+        if (lost && threadIdx.x == 0) mbar_wait(&bar, phase, nullptr);   // bounded drain
+    }
+    (void)lost;
     if constexpr (MODE == X3_RHS_VG) {
         __syncthreads();
         double* scratch = reinterpret_cast<double*>(smraw + P::STAGE + P::TILE);

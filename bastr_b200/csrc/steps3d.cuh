@@ -61,7 +61,7 @@ cudaError_t l3_xpass(bastr_handle* h, const void* MB, void* MC, const double* pi
                        : MODE == X3_TO_PHYS ? mix * 3 * cs + phys : phys + mix * 3 * cs;
         ProfScope ps(h, MODE == X3_RHS_VG ? "k3d_xpass_vg" : MODE == X3_RHS ? "k3d_xpass" : "k3d_xpass_state", b);
         LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MB, (cplx<T>*)MC, pin, pout, vg, h->g,
-                                                twp<T>(h->tw[0])));
+                        twp<T>(h->tw[0]), h->tm3[MODE == X3_RHS_VG ? TM_X3MB13 : TM_X3MB9]));
     });
     return cudaGetLastError();
 }

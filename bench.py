@@ -371,6 +371,7 @@ def e2e_measure(wl, prec, steps, device):
     for p, c in zip(pinned, u):
         p.numpy()[...] = c
     host = [p.numpy() for p in pinned]
+    host_out = [torch.empty(c.shape, dtype=torch.float64, pin_memory=True).numpy() for c in u]
     s.set_state(host)
     s.step(3, shells=True)   # warm-up
     torch.cuda.synchronize()
@@ -378,7 +379,7 @@ def e2e_measure(wl, prec, steps, device):
     s.set_state(host)
     for _ in range(steps):
         s.step(1, shells=True)
-    out = s.get_state()
+    out = s.get_state(out=host_out)
     t1 = time.perf_counter()
     state_bytes = sum(c.nbytes for c in u)
     rec_bytes = 8 * 16 + 2 * (s.allkmax + 1) * 8
@@ -388,7 +389,8 @@ def e2e_measure(wl, prec, steps, device):
             "h2d_bytes_per_step": int(state_bytes / steps),
             "d2h_bytes_per_step": int(rec_bytes + state_bytes / steps),
             "note": "per step: bastr_step(1) with its scalar record and shell spectra read back; "
-                    "field uploaded from pinned memory once and downloaded once per timed run"}
+                    "field uploaded from pinned memory once and downloaded into pinned memory once per "
+                    "timed run"}
 
 
 def oracle_for(wl):

@@ -265,11 +265,12 @@ BASTR_API int bastr_ensemble_run(bastr_ensemble* e, int32_t nsteps, int32_t batc
 
 /* ------------------------------------------------------------------------------------------
  * Learned subgrid closure for a coarse 3D solve (no reference counterpart).  A local network
- * (3x3x3 stencil 3->32, then 1x1x1 32->32, 32->32, 32->3; GELU; BF16 weights, FP32 sums)
- * maps the velocity u [3][nz][ny][nx] to the subgrid term tau.  Device pointers; weights are
- * bastr_net_nparams() BF16 values (uint16_t bit patterns) with FP32 master copies for training.
+ * (3x3x3 stencil 3->32, then 1x1x1 32->32, 32->32, 32->3; GELU; BF16 weights and layer
+ * inputs, FP32 sums) maps the velocity u [3][nz][ny][nx] to the subgrid term tau.  Device
+ * pointers; weights are bastr_net_nparams() BF16 values (uint16_t bit patterns) with FP32 master
+ * copies for training.  Grids of 3 nx ny nz >= 2^31 points return BASTR_E_UNSUPPORTED.
  *
- *   bastr_net_forward   out = scale * net(u)
+ *   bastr_net_forward   out = scale * net(u), the four layers as tensor-core (tcgen05) GEMMs
  *   bastr_net_grad      loss = mean((net(u) - tau)^2) and its gradient; d_part: workspace of
  *                       nblk * (nparams + 1) floats (nblk: e.g. bastr_net_grad_blocks()); the
  *                       result is deterministic for a given nblk

@@ -185,7 +185,7 @@ def test_closure_study_runs_from_ensemble_data(gpu_lib):
     from bastr_b200.closure_study import run
     args = argparse.Namespace(fine=64, ratio=4, reynolds=40.0, dt=1e-3, target=1.5, k0=3.0, train_seeds=[0, 1],
                               test_seed=7, spinup=20, every=10, snapshots=2, steps=20, iters=60, lr=2e-3,
-                              net_seed=0, batch=10, closure_every=1)
+                              net_seed=0, batch=10, closure_every=1, group=1)
     res = run(args)
     assert res["pairs"] == 4 and res["training_data"].startswith("batched solver")
     assert res["loss_last"] < res["loss_first"]
