@@ -46,6 +46,7 @@ EXPORTED = [
     "bastr_closure_apply", "bastr_transfer", "bastr_hitgen",
     "bastr_h5_write", "bastr_h5_read", "bastr_h5_write_field", "bastr_h5_read_field", "bastr_h5_last_error",
     "bastr_subgrid", "bastr_ensemble_subgrid", "bastr_ensemble_run",
+    "bastr_fft_lines", "bastr_slab_pack", "bastr_slab_unpack",
 ]
 BASTR_H5_F64 = 0
 BASTR_H5_I32 = 1
@@ -117,6 +118,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.bastr_last_error.argtypes = [P, C.c_char_p, C.c_int32]
     lib.bastr_profile.argtypes = [P, C.c_int32, C.POINTER(CKernelStat), C.c_int32, C.POINTER(C.c_int32)]
     lib.bastr_spectra_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P, P, P]
+    lib.bastr_fft_lines.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, P]
+    lib.bastr_slab_pack.argtypes = [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P]
+    lib.bastr_slab_unpack.argtypes = [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P]
     lib.bastr_set_plan.argtypes = [P, C.c_int32]
     lib.bastr_ensemble_create.argtypes = [C.POINTER(CParams), C.c_int32, C.POINTER(P)]
     lib.bastr_ensemble_destroy.argtypes = [P]

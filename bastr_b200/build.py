@@ -26,7 +26,7 @@ _COMMON = ["handle.cuh", "solver.cuh", "fft_engine.cuh", "regfft.cuh", "tma.cuh"
 # translation unit -> the sources it includes
 UNITS = {
     "capi.cu": _COMMON + ["diag.cu", "fullfft.cu", "closure.cu", "transfer.cu", "hitgen.cu", "subgrid.cu",
-                         "ensemble.cu"],
+                         "ensemble.cu", "slab.cu"],
     "steps2d_f32.cu": _COMMON + ["pass2d.cu", "steps2d.cuh"],
     "steps2d_f64.cu": _COMMON + ["pass2d.cu", "steps2d.cuh"],
     "steps3d_f32.cu": _COMMON + ["pass2d.cu", "pass3d.cu", "steps3d.cuh"],

@@ -367,10 +367,12 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
                         encode_map(&h->tm[TM_YMB32], h->mb, 4, 3, dy, sy32, by, 0) &&
                         encode_map(&h->tm[TM_YMB64], h->mb, 8, 3, dy, sy64, by, 64);
         if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a mixed-field tensor map");
-    } else if (cs == sizeof(float2) && K <= 256) {
-        // TMA tensor maps of MB [z][kx][f][y] for the FP32 3D x pass (see TensorMapSlot3): FP32
-        // values, 4 consecutive y (32 bytes) x every field x every kx x 1 z plane, 32-byte swizzle
-        const uint64_t NY = g.ny, KK = K, NZ = g.nz;
+    } else if (cs == sizeof(float2) && K <= 256 && g.KY <= 256) {
+        // TMA tensor maps of the FP32 3D passes (see TensorMapSlot3): MB [z][kx][f][y] for the x
+        // pass (4 consecutive y x every field x every kx x 1 z plane, 32-byte swizzle) and
+        // MA [kx][kyi][f][z] for the y-inverse pass (4 consecutive z x every field and one more x
+        // every kyi x 1 kx, 32-byte swizzle)
+        const uint64_t NY = g.ny, KK = K, NZ = g.nz, KY = g.KY;
         bool ok = true;
         const int fins[2] = {9, 13};
         for (int m = 0; m < 2; ++m) {
@@ -378,6 +380,13 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
             const uint64_t dm[4] = {2 * NY, F, KK, NZ}, sm[3] = {NY * 8, F * NY * 8, KK * F * NY * 8};
             const uint32_t bx[4] = {8, (uint32_t)F, (uint32_t)KK, 1};
             ok = ok && encode_map(&h->tm3[m], h->mb, 4, 4, dm, sm, bx, 32);
+        }
+        const int finy[2] = {6, 10};
+        for (int m = 0; m < 2; ++m) {
+            const uint64_t F = finy[m];
+            const uint64_t dm[4] = {2 * NZ, F, KY, KK}, sm[3] = {NZ * 8, F * NZ * 8, KY * F * NZ * 8};
+            const uint32_t bx[4] = {8, (uint32_t)F + 1, (uint32_t)KY, 1};   // one field past MA's: zeros
+            ok = ok && encode_map(&h->tm3[TM_Y3MA6 + m], h->ma, 4, 4, dm, sm, bx, 32);
         }
         if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a 3D mixed-field tensor map");
     }
@@ -455,6 +464,7 @@ int bastr_destroy(bastr_handle* h) {
 }
 
 int bastr_set_state(bastr_handle* h, const double* u1, const double* u2, const double* u3) {
+    NvtxRange range("bastr_set_state");
     if (!h || !u1 || !u2 || (h->g.d == 3 && !u3)) return fail(h, BASTR_E_INVALID, "null field pointer");
     CK(cudaSetDevice(h->device));
     const size_t npts = (size_t)h->g.nx * h->g.ny * h->g.nz;
@@ -472,6 +482,7 @@ int bastr_set_state(bastr_handle* h, const double* u1, const double* u2, const d
 }
 
 int bastr_get_state(bastr_handle* h, double* u1, double* u2, double* u3) {
+    NvtxRange range("bastr_get_state");
     if (!h || !u1 || !u2 || (h->g.d == 3 && !u3)) return fail(h, BASTR_E_INVALID, "null field pointer");
     if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
     CK(cudaSetDevice(h->device));
@@ -601,6 +612,7 @@ int bastr_set_plan(bastr_handle* h, int32_t share_log2) {
 }
 
 int bastr_step_async(bastr_handle* h, int32_t nsteps) {
+    NvtxRange range("bastr_step");
     if (!h || nsteps < 0) return fail(h, BASTR_E_INVALID, "nsteps");
     if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
     if (nsteps > kChunk) return fail(h, BASTR_E_INVALID, "bastr_step_async: at most %d steps per call", kChunk);
@@ -1043,6 +1055,7 @@ int bastr_subgrid(bastr_handle* h, int32_t r, float* d_ubar, float* d_tau) {
 // One closure sub-step on a 3D handle's state: u <- u - dt * scale * net(u) in physical space,
 // then back to the (dealiased) spectral state.
 int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float scale, double dt) {
+    NvtxRange range("bastr_closure_apply");
     if (!h || !d_w) return BASTR_E_INVALID;
     if (h->g.d != 3) return fail(h, BASTR_E_UNSUPPORTED, "the closure network is three-dimensional");
     if (!h->have_state) return fail(h, BASTR_E_STATE, "no state set");
@@ -1066,3 +1079,4 @@ int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float scale, doubl
 }  // extern "C"
 
 #include "ensemble.cu"
+#include "slab.cu"

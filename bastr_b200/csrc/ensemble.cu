@@ -195,6 +195,7 @@ int bastr_ensemble_get_state(bastr_ensemble* e, int32_t i, double* u1, double* u
 // out: [n_real][nsteps] records (realization-major).  Returns BASTR_E_NAN if some realization's
 // Es+Ed became NaN (all records are filled; the message names the first one).
 int bastr_ensemble_step(bastr_ensemble* e, int32_t nsteps, bastr_step_out* out) {
+    NvtxRange range("bastr_ensemble_step");
     if (!e || nsteps < 0 || nsteps > kChunk) return efail(e, BASTR_E_INVALID, "nsteps must be in [0, %d]", kChunk);
     for (size_t i = 0; i < e->hs.size(); ++i)
         if (!e->hs[i]->have_state) return efail(e, BASTR_E_STATE, "realization %zu: no state set", i);
@@ -222,6 +223,7 @@ int bastr_ensemble_step(bastr_ensemble* e, int32_t nsteps, bastr_step_out* out) 
 // device with events on the ensemble's stream around all of them; only the last batch's records
 // stay (bastr_ensemble_step reads them for a batch).  device_ms: total device time.
 int bastr_ensemble_run(bastr_ensemble* e, int32_t nsteps, int32_t batch, double* device_ms) {
+    NvtxRange range("bastr_ensemble_run");
     if (!e || batch < 1 || batch > kChunk || nsteps < 0 || nsteps % batch)
         return efail(e, BASTR_E_INVALID, "nsteps must be a multiple of batch, batch in [1, %d]", kChunk);
     for (size_t i = 0; i < e->hs.size(); ++i)

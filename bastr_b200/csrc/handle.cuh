@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/bastr_gpu.h"
+#include <nvtx3/nvToolsExt.h>
 #ifndef BASTR_PDL
 #define BASTR_PDL 1
 #endif
@@ -118,7 +119,7 @@ struct bastr_handle {
     std::vector<int64_t> ecount;
     // TMA tensor maps of the mixed-field buffers (2D, compute precision), built at creation
     CUtensorMap tm[5] = {};
-    CUtensorMap tm3[2] = {};
+    CUtensorMap tm3[4] = {};
 };
 
 namespace bastr_impl {
@@ -135,8 +136,10 @@ enum Ticket : int { T_SPECTRA = 0, T_HALT = 1, T_ERR = 2, kTickets = 4 };
 // and of a 3D handle whose x pass stages with TMA (FP32, one warp's worth of threads per row):
 //   TM_X3MB9/13      MB [z][kx][f][y] of the product fields (9) / with the velocity-gradient
 //                    fields (13), FP32 values; box = 4 consecutive y x every f x every kx x 1 z
+//   TM_Y3MA6/10      MA [kx][kyi][f][z] of the y-inverse pass's inputs (6 / 10 fields), FP32;
+//                    box = 4 consecutive z x (fields + 1, the last read as zeros) x every kyi x 1 kx
 enum TensorMapSlot : int { TM_XA4 = 0, TM_XA8 = 1, TM_XB8 = 2, TM_YMB32 = 3, TM_YMB64 = 4, kTensorMaps = 5 };
-enum TensorMapSlot3 : int { TM_X3MB9 = 0, TM_X3MB13 = 1 };
+enum TensorMapSlot3 : int { TM_X3MB9 = 0, TM_X3MB13 = 1, TM_Y3MA6 = 2, TM_Y3MA10 = 3 };
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point (no link to libcuda).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -199,11 +202,34 @@ inline bool is_pow2(int n) { return n >= 16 && n <= 2048 && (n & (n - 1)) == 0; 
 
 // Brackets one kernel launch with CUDA events when profiling is on; `bytes` is the launch's
 // algorithmic traffic (unique global reads plus writes of its inputs and outputs).
+// Tracing: every pass launch, step batch and state transfer is an NVTX range named after it
+// (header-only NVTX; the calls cost nothing measurable when no tool is attached).
+#ifndef BASTR_NVTX
+#define BASTR_NVTX 1
+#endif
+struct NvtxRange {
+    explicit NvtxRange(const char* name) {
+#if BASTR_NVTX
+        nvtxRangePushA(name);
+#else
+        (void)name;
+#endif
+    }
+    ~NvtxRange() {
+#if BASTR_NVTX
+        nvtxRangePop();
+#endif
+    }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 struct ProfScope {
     bastr_handle* h;
     size_t ev = 0;
     bool on = false;
-    ProfScope(bastr_handle* hh, const char* name, double bytes) : h(hh) {
+    NvtxRange range;
+    ProfScope(bastr_handle* hh, const char* name, double bytes) : h(hh), range(name) {
         if (!h->prof_on || h->ev_used + 2 > h->ev_pool.size()) return;
         ev = h->ev_used;
         h->ev_used += 2;

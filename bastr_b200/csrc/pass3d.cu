@@ -18,6 +18,21 @@
 #include "solver.cuh"
 #include "tma.cuh"
 
+// Units of the 3D x pass's inverse transforms that share one shared-memory exchange (the rest
+// run as further transforms through the same buffer), and the blocks per SM asked of the
+// register allocator for the FP32 product passes (0: no request).
+#ifndef BASTR_X3_ZA
+#define BASTR_X3_ZA 8
+#endif
+#ifndef BASTR_MINB_X3
+#define BASTR_MINB_X3 0
+#endif
+// Line pairing of the 3D x and y-inverse passes (0: one line per warp; 1: a line per half-warp;
+// 2: lines alternating every 8 lanes, the fastest at 256^3 FP32).
+#ifndef BASTR_X3_PAIR
+#define BASTR_X3_PAIR 2
+#endif
+
 namespace bastr {
 
 // Passes that hold many units at once use 32 bytes per unit per thread.
@@ -152,16 +167,29 @@ template <typename T, int NY, int SET> struct YInv3D {
     static constexpr int G = groups_per_block<FFT::NTR>() > 16 ? 16 : groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
     static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
-    // staging [kyi][f][line] of KY modes x FIN fields, sized at run time
+    // lines served in pairs by pairs of warps, as in the x pass (one warp's worth of threads per
+    // line, an even number of lines, exchange buffers a multiple of 128 bytes long)
+    static constexpr bool PAIRED = BASTR_X3_PAIR > 0 && FFT::NTR == 32 && G % 2 == 0 &&
+                                   (FFT::SMEM_ELEMS * (int)sizeof(cplx<T>)) % 128 == 0;
+    // TMA staging of the product fields (FP32): the group's [kyi][f][4 lines] values as one box of
+    // a 4-D tensor map over MA (KY < NY <= 256 modes in one box) with the 32-byte swizzle and one
+    // field more than MA holds (read as zeros), an odd number of 32-byte rows per mode: a model of
+    // the banks gives conflict-free 8-byte reads for the paired lines (the dense unswizzled layout
+    // of 6 or 10 fields is 8-way conflicted)
+    static constexpr bool TMA = PAIRED && sizeof(T) == 4 && G == 4 && SET != YB_STATE && NY <= 256;
+    static constexpr int FB = TMA ? FIN + 1 : FIN;                 // staged fields per mode
+    // staging [kyi][f][line] of KY modes x FB fields, sized at run time
     __host__ __device__ static size_t stage_bytes(int KY) {
-        return ((size_t)G * KY * FIN * sizeof(cplx<T>) + 15) & ~(size_t)15;
+        const size_t b = (size_t)G * KY * FB * sizeof(cplx<T>);
+        return TMA ? 1024 + ((b + 1023) & ~(size_t)1023) : (b + 15) & ~(size_t)15;
     }
     static size_t smem(int KY) { return stage_bytes(KY) + XCH; }
 };
 
 template <typename T, int NY, int SET>
 __global__ void __launch_bounds__(YInv3D<T, NY, SET>::NT)
-k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const cplx<T>* __restrict__ tw) {
+k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const cplx<T>* __restrict__ tw,
+         const __grid_constant__ CUtensorMap tma_map) {
     pdl_wait();
     if (halted(g)) return;
     using P = YInv3D<T, NY, SET>;
@@ -169,14 +197,38 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
     constexpr int EPT = P::EPT, UG = P::UG, F = P::F, FIN = P::FIN, G = P::G;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
-    const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
+    // line of this thread: pairs of lines served by pairs of warps, alternating every 8 lanes
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int gi = !P::PAIRED ? threadIdx.x / FFT::NTR
+                 : BASTR_X3_PAIR == 1 ? 2 * (wp >> 1) + ((wp & 1) ^ (lane >> 4))
+                                      : 2 * (wp >> 1) + (((lane >> 3) & 1) ^ (wp & 1));
+    const int t = P::PAIRED ? lane : threadIdx.x % FFT::NTR;
     const int K = g.K, KY = g.KY, NZ = g.nz;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::stage_bytes(KY)) + gi * FFT::SMEM_ELEMS;
     const int nlines = K * NZ;                 // line = kx*NZ + z
     const int nitems = (nlines + G - 1) / G;
+    // TMA tile at the first 1024-byte boundary of the staging area
+    unsigned char* tmat = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    __shared__ __align__(8) uint64_t bar;
+    if constexpr (P::TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    uint32_t phase = 0;
+    bool lost = false;   // a TMA completion wait gave up (recorded in g.err)
     auto issue = [&](int item) {
         // gather [kyi][f][z] from MA[kx][kyi][f][z]: G consecutive z per (kyi, f)
         const int l0 = item * G, kx0 = l0 / NZ, z0 = l0 - kx0 * NZ;
+        if constexpr (P::TMA) {
+            if (threadIdx.x == 0) {
+                mbar_expect_tx(&bar, (uint32_t)(G * KY * P::FB * (int)sizeof(cplx<T>)));
+                tma_load_4d(tmat, &tma_map, 2 * z0, 0, 0, kx0, &bar);
+            }
+            return;
+        }
         constexpr int RB = G * (int)sizeof(cplx<T>);
         constexpr int CH = RB % 16 == 0 ? 16 : 8;
         constexpr int NCH = RB / CH;
@@ -194,8 +246,17 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
     int item = blockIdx.x;
     if (item < nitems) issue(item);
     for (; item < nitems; item += gridDim.x) {
-        cp_async_wait<0>();
-        __syncthreads();
+        if constexpr (P::TMA) {
+            const bool ok = mbar_wait(&bar, phase, g.err);
+            if (__syncthreads_or(!ok)) {   // block-uniform: stop, and drain below
+                lost = true;
+                break;
+            }
+            phase ^= 1u;
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         const int l = item * G + gi;
         const bool valid = l < nlines;
         const int kx = l / NZ, z = l - kx * NZ;
@@ -213,7 +274,12 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
                 if (valid && kyi >= 0) {
                     const T ky = (T)trunc_k(kyi, K, KY);
                     const cplx<T>* src0 = line + (size_t)kyi * FIN * G;
-                    auto src = [&](int fi) { return src0[fi * G]; };
+                    auto src = [&](int fi) -> cplx<T> {
+                        if constexpr (P::TMA)
+                            return *reinterpret_cast<const cplx<T>*>(
+                                tmat + swz<32>((uint32_t)((kyi * P::FB + fi) * G + gi) * (uint32_t)sizeof(cplx<T>)));
+                        else return src0[fi * G];
+                    };
                     if constexpr (SET == YB_STATE) {
                         f[0] = src(0); f[1] = src(1); f[2] = src(2);
                     } else {
@@ -253,6 +319,10 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
         }
     }
     cp_async_wait<0>();
+    if constexpr (P::TMA) {
+        if (lost && threadIdx.x == 0) mbar_wait(&bar, phase, nullptr);   // bounded drain
+    }
+    (void)lost;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -260,20 +330,6 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
 // ---------------------------------------------------------------------------------------
 enum X3Mode : int { X3_RHS = 1, X3_RHS_VG = 2, X3_TO_PHYS = 3, X3_FROM_PHYS = 4 };
 
-// Units of the 3D x pass's inverse transforms that share one shared-memory exchange (the rest
-// run as further transforms through the same buffer), and the blocks per SM asked of the
-// register allocator for the FP32 product passes (0: no request).
-#ifndef BASTR_X3_ZA
-#define BASTR_X3_ZA 8
-#endif
-#ifndef BASTR_MINB_X3
-#define BASTR_MINB_X3 0
-#endif
-// Row pairing of the 3D x pass (0: one row per warp; 1: a row per half-warp; 2: rows alternating
-// every 8 lanes, the fastest at 256^3 FP32: 2.50 -> 2.47 ms per step).
-#ifndef BASTR_X3_PAIR
-#define BASTR_X3_PAIR 2
-#endif
 
 template <typename T, int NX, int MODE> struct XPass3D {
     static constexpr int FIN = MODE == X3_RHS ? 9 : MODE == X3_RHS_VG ? 13 : MODE == X3_TO_PHYS ? 3 : 0;

@@ -41,7 +41,8 @@ cudaError_t l3_yinv(bastr_handle* h, const void* MA, void* MB) {
         const double cs = sizeof(cplx<T>);
         ProfScope ps(h, SET == YB_RHS_VG ? "k3d_yinv_vg" : "k3d_yinv",
                      (double)h->g.K * h->g.nz * (h->g.KY * P::FIN + h->g.ny * P::F) * cs);
-        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<T>*)MA, (cplx<T>*)MB, h->g, twp<T>(h->tw[1])));
+        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<T>*)MA, (cplx<T>*)MB, h->g, twp<T>(h->tw[1]),
+                        h->tm3[SET == YB_RHS_VG ? TM_Y3MA10 : TM_Y3MA6]));
     });
     return cudaGetLastError();
 }

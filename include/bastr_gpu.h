@@ -300,6 +300,27 @@ BASTR_API int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float sc
 BASTR_API int bastr_subgrid(bastr_handle* h, int32_t r, float* d_ubar, float* d_tau);
 BASTR_API int bastr_ensemble_subgrid(bastr_ensemble* e, int32_t i, int32_t r, float* d_ubar, float* d_tau);
 
+/* ------------------------------------------------------------------------------------------
+ * Slab-decomposed 3D transforms over several GPUs: the reference distributes its grid in z-slabs
+ * over MPI ranks and transforms it with FFTW-MPI (decomposition fftwlink.F90:63-77, transforms
+ * fftwlink.F90:324-368); these are the per-GPU pieces, on caller-owned device arrays, between
+ * which the caller runs one all-to-all of equal blocks per transform (bastr_b200/slabfft.py:
+ * NCCL).  Complex FP64 arrays [nz][ny][nx] (x fastest), device pointers, the caller's stream.
+ *
+ *   bastr_fft_lines    every line along `axis` (0 x, 1 y, 2 z) transformed in place: dir -1
+ *                      e^{-ikx}, dir +1 e^{+ikx}, times `scale`; line lengths powers of two in
+ *                      [16, 2048]; the first call per (device, length) makes a twiddle table
+ *                      (cudaMalloc) kept until exit
+ *   bastr_slab_pack    d_blocks[q][zl][yl][x] = d_slab[zl][q*nyl + yl][x], nyl = ny/nparts
+ *   bastr_slab_unpack  its inverse
+ * ------------------------------------------------------------------------------------------ */
+BASTR_API int bastr_fft_lines(double* d_a, int32_t nx, int32_t ny, int32_t nz, int32_t axis, int32_t dir,
+                              double scale, void* stream);
+BASTR_API int bastr_slab_pack(const double* d_slab, double* d_blocks, int32_t nx, int32_t ny, int32_t nzl,
+                              int32_t nparts, void* stream);
+BASTR_API int bastr_slab_unpack(const double* d_blocks, double* d_slab, int32_t nx, int32_t ny, int32_t nzl,
+                                int32_t nparts, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
