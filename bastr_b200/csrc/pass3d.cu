@@ -356,10 +356,11 @@ template <typename T, int NX, int MODE> struct XPass3D {
     // per row, an even number of rows and exchange buffers a multiple of 128 bytes long
     static constexpr bool PAIRED = BASTR_X3_PAIR > 0 && NTR == 32 && G % 2 == 0 &&
                                    (IFFT::SMEM_ELEMS * (int)sizeof(cplx<T>)) % 128 == 0;
-    // tile elements per kx, odd in FP32 so that the split's stores of consecutive kx spread over
-    // the banks (an even stride that is conflict-free for paired rows measured slower: it pushed
-    // the velocity-gradient variant past its shared-memory budget)
-    static constexpr int TSTR = sizeof(T) == 4 ? ((3 * G) | 1) : 3 * G;
+    // tile elements per kx in FP32: for paired rows an even stride twice an odd number (the two
+    // rows on opposite bank parities: conflict-free split stores), otherwise odd; the
+    // velocity-gradient variant keeps the odd one, since two more elements per kx would leave it
+    // one block per SM
+    static constexpr int TSTR = sizeof(T) != 4 ? 3 * G : (PAIRED && MODE == X3_RHS) ? 3 * G + 2 : ((3 * G) | 1);
     // TMA staging (the FP32 product passes with paired rows): the row group's [kx][f][4 rows]
     // values as one box of a 4-D tensor map over MB, unpadded and swizzled at 32 bytes, which
     // keeps the paired rows' 8-byte reads conflict-free; one elected thread issues it
@@ -647,8 +648,13 @@ template <typename T, int NY> struct YFwd3D {
     static constexpr int G = groups_per_block<FFT::NTR>() > 16 ? 16 : groups_per_block<FFT::NTR>();
     static constexpr int NT = G * FFT::NTR;
     static constexpr size_t STAGE = (size_t)G * NY * 3 * sizeof(cplx<T>);
-    static constexpr size_t TILE = (size_t)NY * G * 3 * sizeof(cplx<T>);   // output tile [kyi][line][c]
-    static constexpr size_t SMEM = STAGE + TILE + (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    // output tile [kyi][line][c] of the KY kept modes, TS elements per mode: an odd number in
+    // FP32, so that the 8-byte stores of consecutive kyi by a warp reach distinct banks
+    // (G*3 = 12 elements gave 4-way conflicts), sized at run time
+    static constexpr int TS = sizeof(T) == 4 ? ((G * 3) | 1) : G * 3;
+    __host__ __device__ static size_t tile_bytes(int KY) { return (((size_t)KY * TS * sizeof(cplx<T>)) + 15) & ~(size_t)15; }
+    static constexpr size_t XCH = (size_t)G * FFT::SMEM_ELEMS * sizeof(cplx<T>);
+    static size_t smem(int KY) { return STAGE + tile_bytes(KY) + XCH; }
 };
 
 template <typename T, int NY>
@@ -663,8 +669,8 @@ k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const 
     cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw);
     cplx<T>* tile = reinterpret_cast<cplx<T>*>(smraw + P::STAGE);
     const int gi = threadIdx.x / FFT::NTR, t = threadIdx.x % FFT::NTR;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::TILE) + gi * FFT::SMEM_ELEMS;
     const int K = g.K, KY = g.KY, NZ = g.nz;
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::tile_bytes(KY)) + gi * FFT::SMEM_ELEMS;
     const int nlines = K * NZ;                 // line = kx*NZ + z
     const int nitems = (nlines + G - 1) / G;
     auto issue = [&](int item) {
@@ -699,7 +705,7 @@ k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const 
         for (int e = 0; e < EPT; ++e) {
             const int kyi = pos_trunc(FFT::out_pos(t, e), K, KY, NY);
             if (kyi < 0) continue;
-            cplx<T>* dst = tile + ((size_t)kyi * G + gi) * 3;
+            cplx<T>* dst = tile + (size_t)kyi * P::TS + gi * 3;
 #pragma unroll
             for (int c = 0; c < 3; ++c) dst[c] = v[c * EPT + e];
         }
@@ -709,7 +715,7 @@ k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const 
             const int l0 = item * G, kx0 = l0 / NZ, z0 = l0 - kx0 * NZ;
             for (int i = threadIdx.x; i < KY * G * 3; i += P::NT) {
                 const int kyi = i / (G * 3), rem = i - kyi * (G * 3);
-                MD[(((size_t)kx0 * KY + kyi) * NZ + z0) * 3 + rem] = tile[i];
+                MD[(((size_t)kx0 * KY + kyi) * NZ + z0) * 3 + rem] = tile[(size_t)kyi * P::TS + rem];
             }
         }
     }

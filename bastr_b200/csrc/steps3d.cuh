@@ -72,11 +72,12 @@ cudaError_t l3_yfwd(bastr_handle* h, const void* MC, void* MD) {
     SIZE_CASES3(h->g.ny, {
         using P = YFwd3D<T, NN>;
         auto k = k3d_yfwd<T, NN>;
+        const size_t smem = P::smem(h->g.KY);
         int grid = 1;
-        cudaError_t e = persistent_grid(h, k, P::SMEM, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
+        cudaError_t e = persistent_grid(h, k, smem, P::NT, cdiv(h->g.K * h->g.nz, P::G), &grid);
         if (e != cudaSuccess) return e;
         ProfScope ps(h, "k3d_yfwd", (double)h->g.K * h->g.nz * (h->g.ny + h->g.KY) * 3 * sizeof(cplx<T>));
-        LAUNCH(launch_k(h, k, grid, P::NT, P::SMEM, (const cplx<T>*)MC, (cplx<T>*)MD, h->g, twp<T>(h->tw[1])));
+        LAUNCH(launch_k(h, k, grid, P::NT, smem, (const cplx<T>*)MC, (cplx<T>*)MD, h->g, twp<T>(h->tw[1])));
     });
     return cudaGetLastError();
 }
