@@ -597,169 +597,6 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
 }
 
 // ---------------------------------------------------------------------------------------
-// Pass B, product only, one inverse transform at a time (BASTR_XPASS_SEQ).
-// ---------------------------------------------------------------------------------------
-// The same x pass as k2d_xpass<XM_RHS> (same transforms, same product, same output), with the
-// three packed inverse transforms run one after another: u = (u1, u2) first, then (d1 u1, d1 u2)
-// whose products with u1 start N, then (d2 u1, d2 u2) which complete it.  A thread holds at most
-// u, N and one transform's values instead of all three transforms', and the exchange buffer holds
-// one line instead of three, so more blocks fit on an SM; the records of the row come by TMA into
-// one of two tiles, so the next row's copy overlaps the whole of this row's work.
-#ifndef BASTR_XPASS_SEQ
-#define BASTR_XPASS_SEQ 0
-#endif
-#ifndef BASTR_MINB_XSEQ
-#define BASTR_MINB_XSEQ 3
-#endif
-
-template <typename T, int NX> struct XSeq2D {
-    static constexpr int EPT = ept_fit<NX, sizeof(T) == 8 ? EptOf<T>::v : BASTR_EPT_XPASS_F32>();
-    using IFFT = RegFFT<T, NX, EPT, 1, true>;
-    using FFFT = RegFFT<T, NX, EPT, 1, false>;
-    static constexpr int NTR = IFFT::NTR;
-    static constexpr int NT = NTR;
-    static constexpr bool OK = NTR >= 64;          // one row per block of at least two warps
-    static constexpr int MINB = sizeof(T) == 4 ? BASTR_MINB_XSEQ : 1;
-    static constexpr int KMAX = NX / 3;
-    static constexpr int RB = 4 * (int)sizeof(cplx<T>);   // record of (g1, h1, g2, h2)
-    static constexpr int SWZA = RB;
-    static constexpr int BK = KMAX < 256 ? KMAX : 256;
-    static constexpr int NBOX = (KMAX + BK - 1) / BK;
-    static constexpr size_t TILEA = ((size_t)NBOX * BK * RB + 1023) & ~(size_t)1023;
-    static constexpr uint32_t TX_BYTES = (uint32_t)(NBOX * BK * RB);
-    static constexpr size_t STAGE = 1024 + 2 * TILEA;
-    static constexpr size_t XCH = (size_t)IFFT::SMEM_ELEMS * sizeof(cplx<T>);
-    static constexpr size_t XCHR = XCH > (size_t)9 * NT * 8 ? XCH : (size_t)9 * NT * 8;
-    static constexpr size_t TWB = BASTR_XPASS_TW_SMEM ? tw_stage_bytes<T, IFFT, FFFT>() : 0;
-    static constexpr size_t SMEM = STAGE + XCHR + TWB;
-};
-
-template <typename T, int NX>
-__global__ void __launch_bounds__(XSeq2D<T, NX>::NT, XSeq2D<T, NX>::MINB)
-k2d_xpass_seq(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const cplx<T>* tw,
-              const __grid_constant__ CUtensorMap tmA) {
-    using P = XSeq2D<T, NX>;
-    using IFFT = typename P::IFFT;
-    using FFFT = typename P::FFFT;
-    constexpr int EPT = P::EPT, NTR = P::NTR;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    unsigned char* tile0 = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw + P::STAGE);
-    __shared__ __align__(8) uint64_t bar[2];
-    const int t = threadIdx.x;
-    constexpr bool STW = P::TWB > 0;
-    const cplx<T>* twi = tw;
-    const cplx<T>* twf = tw;
-    if constexpr (STW) {
-        cplx<T>* d = reinterpret_cast<cplx<T>*>(smraw + P::STAGE + P::XCHR);
-        IFFT::fill_stage_twiddles(d, tw);
-        FFFT::fill_stage_twiddles(d + IFFT::TWS_ELEMS, tw);
-        twi = d;
-        twf = d + IFFT::TWS_ELEMS;
-    }
-    pdl_wait();
-    if (halted(g)) return;
-    const int K = g.K, NY = g.ny;
-    if (t == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    uint32_t phase[2] = {0, 0};
-    auto issue = [&](int y0, int buf) {
-        if (t == 0) {
-            unsigned char* tile = tile0 + (size_t)buf * P::TILEA;
-            mbar_expect_tx(&bar[buf], P::TX_BYTES);
-#pragma unroll
-            for (int b = 0; b < P::NBOX; ++b)
-                tma_load_4d(tile + (size_t)b * P::BK * P::RB, &tmA, 0, y0, 0, b * P::BK, &bar[buf]);
-        }
-    };
-    // the records of wavenumber k: (g1, h1) in chunk 0..., (g2, h2) after them
-    auto rec = [&](const unsigned char* tile, int k, cplx<T>& g1, cplx<T>& h1, cplx<T>& g2, cplx<T>& h2) {
-        if constexpr (sizeof(T) == 4) {
-            const float4 a = tile_chunk<P::SWZA, P::RB, float4>(tile, k, 0);
-            const float4 b = tile_chunk<P::SWZA, P::RB, float4>(tile, k, 1);
-            g1 = mk<T>(a.x, a.y); h1 = mk<T>(a.z, a.w);
-            g2 = mk<T>(b.x, b.y); h2 = mk<T>(b.z, b.w);
-        } else {
-            g1 = tile_chunk<P::SWZA, P::RB, cplx<T>>(tile, k, 0);
-            h1 = tile_chunk<P::SWZA, P::RB, cplx<T>>(tile, k, 1);
-            g2 = tile_chunk<P::SWZA, P::RB, cplx<T>>(tile, k, 2);
-            h2 = tile_chunk<P::SWZA, P::RB, cplx<T>>(tile, k, 3);
-        }
-    };
-    // unit j of the row at register element e: 0 = (g1, g2), 1 = i kx (g1, g2), 2 = (h1, h2)
-    auto load_unit = [&](const unsigned char* tile, int j, cplx<T>* v) {
-#pragma unroll
-        for (int e = 0; e < EPT; ++e) {
-            const int p = IFFT::in_pos(t, e);
-            const bool lo = p < K, hi = p > NX - K;
-            const int k = lo ? p : NX - p;
-            v[e] = mk<T>(0, 0);
-            if (IFFT::in_band(e, NX / 3 + 1)) continue;
-            if (lo || hi) {
-                cplx<T> g1, h1, g2, h2;
-                rec(tile, k, g1, h1, g2, h2);
-                const bool z0 = p == 0;
-                const T kx = (T)k;
-                v[e] = j == 0 ? pack_at<T>(g1, g2, hi, z0)
-                     : j == 1 ? pack_at<T>(cscale<T>(cmuli<T>(g1), kx), cscale<T>(cmuli<T>(g2), kx), hi, z0)
-                              : pack_at<T>(h1, h2, hi, z0);
-            }
-        }
-    };
-    const int stride = gridDim.x;
-    int y = blockIdx.x, buf = 0;
-    if (y < NY) issue(y, 0);
-    if (y + stride < NY) issue(y + stride, 1);
-    bool lost = false;
-    for (; y < NY; y += stride) {
-        const bool ok = mbar_wait(&bar[buf], phase[buf], g.err);
-        if (__syncthreads_or(!ok)) {
-            lost = true;
-            break;
-        }
-        phase[buf] ^= 1u;
-        const unsigned char* tile = tile0 + (size_t)buf * P::TILEA;
-        cplx<T> u[EPT], n[EPT], v[EPT];
-        load_unit(tile, 0, u);
-        IFFT::template run<STW>(u, sm, twi, t);
-        load_unit(tile, 1, v);
-        IFFT::template run<STW>(v, sm, twi, t);
-#pragma unroll
-        for (int e = 0; e < EPT; ++e) n[e] = mk<T>(-u[e].x * v[e].x, -u[e].x * v[e].y);   // -u1 d1 u_i
-        load_unit(tile, 2, v);
-        __syncthreads();   // this tile is consumed: fetch the row after the next one into it
-        if (y + 2 * stride < NY) issue(y + 2 * stride, buf);
-        IFFT::template run<STW>(v, sm, twi, t);
-        // advective product (solution.F90:841-846): N_i = -(u1 d1 u_i + u2 d2 u_i)
-#pragma unroll
-        for (int e = 0; e < EPT; ++e) n[e] = mk<T>(n[e].x - u[e].y * v[e].x, n[e].y - u[e].y * v[e].y);
-        FFFT::template run<STW>(n, sm, twf, t);
-#pragma unroll
-        for (int e = 0; e < EPT; ++e) {
-            if (FFFT::out_band(e, NX / 3 + 1)) continue;
-            sm[pidx(FFFT::out_pos(t, e))] = n[e];
-        }
-        __syncthreads();
-        for (int k = t; k < K; k += NTR) {
-            const cplx<T> Z = sm[pidx(k)];
-            const cplx<T> Zc = cconj<T>(sm[pidx(k == 0 ? 0 : NX - k)]);
-            st2<T>(MB + (((size_t)(y >> 1) * K + k) * 2 + (y & 1)) * 2, cscale<T>(cadd<T>(Z, Zc), (T)0.5),
-                   cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5));
-        }
-        __syncthreads();   // the exchange buffer is read: the next row's transforms may use it
-        buf ^= 1;
-    }
-    if (lost && t == 0) {   // bounded drains of the copies in flight
-        mbar_wait(&bar[buf], phase[buf], nullptr);
-        mbar_wait(&bar[buf ^ 1], phase[buf ^ 1], nullptr);
-    }
-}
-
-// ---------------------------------------------------------------------------------------
 // Pass C: forward transforms along y of kx columns + spectral epilogue.
 // ---------------------------------------------------------------------------------------
 // TMA staging of the forward y passes (one kx column per block): the column's records of two

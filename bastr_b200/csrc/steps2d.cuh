@@ -30,25 +30,6 @@ cudaError_t l2_yinv(bastr_handle* h, const void* S, void* MA, int ftot) {
 template <typename T, int MODE>
 cudaError_t l2_xpass(bastr_handle* h, const void* MA, int ftot, void* MB, const double* pin, double* pout,
                      double* vg) {
-    if constexpr (MODE == XM_RHS && BASTR_XPASS_SEQ) {
-        // the product pass with one inverse transform at a time, where a row fills two warps
-        cudaError_t r = cudaErrorNotSupported;
-        SIZE_CASES(h->g.nx, {
-            using Q = XSeq2D<T, NN>;
-            if constexpr (Q::OK) {
-                if (sizeof(T) != (h->fp32 ? 4u : 8u)) return cudaErrorInvalidValue;
-                auto k = k2d_xpass_seq<T, NN>;
-                int grid = 1;
-                cudaError_t e = persistent_grid(h, k, Q::SMEM, Q::NT, h->g.ny, &grid);
-                if (e != cudaSuccess) return e;
-                ProfScope ps(h, "k2d_xpass", (double)h->g.ny * h->g.K * 6 * sizeof(cplx<T>));
-                LAUNCH(launch_k(h, k, grid, Q::NT, Q::SMEM, (const cplx<T>*)MA, (cplx<T>*)MB, h->g, twp<T>(h->tw[0]),
-                                h->tm[TM_XA4]));
-                r = cudaSuccess;
-            }
-        });
-        if (r == cudaSuccess) return cudaGetLastError();
-    }
     SIZE_CASES(h->g.nx, {
         using P = XPass2D<T, NN, MODE>;
         auto k = k2d_xpass<T, NN, MODE>;
