@@ -46,6 +46,22 @@ def test_2d_fp64_many_steps(gpu_lib, name, kw, k0):
     _check(err, 1e-9)
 
 
+@pytest.mark.parametrize("dims,kw", [
+    ((128, 128, 0), dict(reynolds=5000.0, deltat=1e-4, timemethod=2, forcemethod=2, forcek=5, target_energy=0.075,
+                         lprojectd=True)),
+    ((32, 32, 32), dict(reynolds=2000.0, deltat=5e-4, timemethod=2, forcemethod=1, target_energy=1.5)),
+], ids=["2d_band_proj", "3d_linear"])
+def test_cn_many_steps(gpu_lib, dims, kw):
+    """Crank-Nicolson (six sweeps per step, solution.F90:205-231, 272-301) over many steps, with
+    forcing: the sweeps' fixed-point iterates stay at FP64 parity."""
+    ia, ja, ka = dims
+    p = make_params(ia, ja, ka, kmax=100, **kw)
+    u = field(ia, ja, ka, k0=4.0 if ka == 0 else 3.0, seed=6)
+    n = 30 if ka == 0 else 20
+    err = compare(run_oracle(p, u, n), run_gpu(p, u, n, "fp64"))
+    _check(err, 1e-9)
+
+
 def test_2d_nonsquare(gpu_lib):
     p = make_params(64, 128, 0, reynolds=3000.0, deltat=1e-4, forcemethod=2, forcek=3, target_energy=0.1)
     u = field(64, 128, 0, k0=3.0, seed=3)
