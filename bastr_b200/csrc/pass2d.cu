@@ -596,6 +596,36 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
     }
 }
 
+// Prefetch of the state a line's epilogue will read (the u0, us and acc values of modes
+// first .. first + n - 1 of each of D components cst elements apart; 2D: interleaved, cst = 1
+// and 2n values), issued before the line's forward transform so that the loads after it find
+// the lines in L2: 0 none, 1 into L1, 2 into L2 with the evict-last priority (the default; 2048^2
+// FP32: 0.372 -> 0.367 ms per step, L1 0.368).
+#ifndef BASTR_EPI_PREFETCH
+#define BASTR_EPI_PREFETCH 2
+#endif
+template <typename T, int D, int EPI>
+__device__ __forceinline__ void epi_prefetch(const StageIO<T>& io, size_t first, int n, size_t cst, bool from_u0,
+                                             int t, int nthreads) {
+    if constexpr (BASTR_EPI_PREFETCH != 0 && EPI != EPI_STORE) {
+        auto pf = [&](const void* base, size_t bytes) {
+            for (size_t off = (size_t)t * 128; off < bytes; off += (size_t)nthreads * 128) {
+                const char* a = static_cast<const char*>(base) + off;
+                if constexpr (BASTR_EPI_PREFETCH == 1) asm volatile("prefetch.global.L1 [%0];" ::"l"(a));
+                else asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(a));
+            }
+        };
+        const int runs = D == 2 ? 1 : D;                       // 2D: one interleaved run
+        const size_t len = D == 2 ? (size_t)n * 2 : (size_t)n;
+#pragma unroll
+        for (int c = 0; c < runs; ++c) {
+            pf(io.u0 + first + c * cst, len * sizeof(double2));
+            if (!from_u0 && EPI != EPI_RK2) pf(io.us + first + c * cst, len * sizeof(cplx<T>));
+            if constexpr (EPI == EPI_RK2 || EPI == EPI_RK3) pf(io.acc + first + c * cst, len * sizeof(cplx<T>));
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // Pass C: forward transforms along y of kx columns + spectral epilogue.
 // ---------------------------------------------------------------------------------------
@@ -727,6 +757,7 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
         }
         __syncthreads();   // the staging buffer is free: fetch the next column group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        if (valid) epi_prefetch<T, 2, EPI>(io, (size_t)kx * KY * 2, KY, 1, input_is_u0 != 0, t, FFT::NTR);
         FFT::template run<STW>(v, sm, tw, t);
         if (valid) {
             const double w = kx == 0 ? 1.0 : 2.0;
@@ -895,6 +926,7 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
         }
         __syncthreads();   // the staging buffer is free: fetch the next column group now
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        if (valid) epi_prefetch<T, 2, EPI>(io, (size_t)kx * KY * 2, KY, 1, input_is_u0 != 0, t, FFT::NTR);
         FFT::template run<STW>(v, sm, twf, t);
         // the next stage input at the positions this thread holds (zero outside the kept set)
         cplx<T> nx[2 * EPT];

@@ -777,6 +777,7 @@ k3d_zfwd(const cplx<T>* __restrict__ MD, StageIO<T> io, int input_is_u0, Geo g, 
         }
         __syncthreads();
         if (item + (int)gridDim.x < nitems) issue(item + gridDim.x);
+        if (valid) epi_prefetch<T, 3, EPI>(io, (size_t)l * KZ, KZ, (size_t)g.ps, input_is_u0 != 0, t, FFT::NTR);
         FFT::run(v, sm, tw, t);
         if (valid) {
             const int ky = trunc_k(kyi, K, KY);
