@@ -118,10 +118,10 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec, bool vg) {
         ProfScope ps(h, "k_force_band", 0);
         if (h->g.d == 2)
             LAUNCH(launch_k(h, k_force_band<2, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
-                            h->rng, vgp, vgn));
+                            h->rng, vgp, vgn, (const int*)h->sp_modes, h->band_lo, h->band_hi));
         else
             LAUNCH(launch_k(h, k_force_band<3, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
-                            h->rng, vgp, vgn));
+                            h->rng, vgp, vgn, (const int*)h->sp_modes, h->band_lo, h->band_hi));
     }
     return cudaGetLastError();
 }
@@ -439,6 +439,10 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
         shell_item[h->nshell] = (int)item_lo.size();
         h->n_items = (int)item_lo.size();
         item_lo.push_back(cnt[h->nshell]);
+        // the band of the band-forcing methods: shell forcek of the list (empty past the last shell)
+        const int fk = p->forcek;
+        h->band_lo = fk >= 1 && fk < h->nshell ? cnt[fk] : cnt[h->nshell];
+        h->band_hi = fk >= 1 && fk < h->nshell ? cnt[fk + 1] : cnt[h->nshell];
         dev_alloc(h, &h->sp_modes, std::max<size_t>(modes.size(), 1) * sizeof(int), st);
         dev_alloc(h, &h->sp_item_lo, item_lo.size() * sizeof(int), st);
         dev_alloc(h, &h->sp_shell_item, shell_item.size() * sizeof(int), st);

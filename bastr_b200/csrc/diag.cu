@@ -14,6 +14,12 @@
 #include <cstdint>
 #include "solver.cuh"
 
+// List entries a thread of the spectra kernel loads together (their index and state loads in
+// flight at once).
+#ifndef BASTR_SPECTRA_U
+#define BASTR_SPECTRA_U 4
+#endif
+
 namespace bastr {
 
 // Record slots (doubles) written per step on the device.
@@ -151,7 +157,7 @@ __global__ void __launch_bounds__(NT) k_spectra_fused(double2* __restrict__ U0, 
     if (halted(g)) return;
     __shared__ double scratch[4 * NT];
     __shared__ unsigned int flag;
-    constexpr int U = 4;
+    constexpr int U = BASTR_SPECTRA_U;
     const int lo = item_lo[blockIdx.x], hi = item_lo[blockIdx.x + 1];
     const double2 pd = pend[0];
     const bool scale = pd.x != 0.0;
@@ -345,130 +351,120 @@ __device__ __forceinline__ double band_phase(int kx, int ky, int kz, unsigned lo
 }
 
 // Band forcing, methods 2-5: the band |kk - forcek| < 1/2 is exactly the shell nint(kk) =
-// forcek.  One block enumerates it.  Methods 2 and 5: f = the band part of u, E = mean(f^2) in
-// fixed order, then u += factor*f.  Methods 3 and 4 (solution.F90:379-482, 631-753): f has
-// unit-amplitude dilatational modes k/|k| (sin phi + i cos phi) with random phases phi; E =
-// mean(f.u), Fen = mean(f^2), energy = mean(|u|^2) (rec[R_ENERGY]); factor = (sqrt(max((target -
-// energy) Fen + E^2, 0)) - E) / Fen (method 3) or target (method 4); u += factor*f.  *rng counts
-// the forcing calls (the random stream's counter).
+// forcek (no integer |k|^2 lies on a half-integer radius), whose kept modes are the entries
+// band_lo .. band_hi-1 of the spectra's shell-sorted mode list; the threads of the one block
+// take one entry each (forcek = 0: the k = 0 mode alone).  Methods 2 and 5: f = the band part of
+// u, E = mean(f^2) in fixed order, then u += factor*f.  Methods 3 and 4 (solution.F90:379-482,
+// 631-753): f has unit-amplitude dilatational modes k/|k| (sin phi + i cos phi) with random
+// phases phi; E = mean(f.u), Fen = mean(f^2), energy = mean(|u|^2) (rec[R_ENERGY]); factor =
+// (sqrt(max((target - energy) Fen + E^2, 0)) - E) / Fen (method 3) or target (method 4);
+// u += factor*f.  *rng counts the forcing calls (the random stream's counter).
 template <int D, int NT>
 __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo g, int method, int forcek,
                                                    double target, int project2d, double* __restrict__ rec,
                                                    unsigned long long* rng, const double* __restrict__ vg_part,
-                                                   int vg_nblk) {
+                                                   int vg_nblk, const int* __restrict__ modes, int band_lo,
+                                                   int band_hi) {
     pdl_wait();
     if (halted(g)) return;
     __shared__ double scratch[7 * NT];
+    __shared__ double s_factor;
     if (vg_nblk > 0) {   // the step's velocity-gradient statistics, as k_force_linear does
         velgrad_finish<NT>(vg_part, vg_nblk, g, rec, scratch);
         __syncthreads();
     }
     const bool rnd = method == 3 || method == 4;
     const unsigned long long ctr = rnd ? *rng : 0ull;
-    const int s = forcek;
-    const int K = g.K;
-    const long long lo = s == 0 ? 0 : (long long)s * s - s + 1;
-    long long hi = s == 0 ? 0 : (long long)s * s + s;
-    const long long K2m1 = (long long)K * K - 1;
-    if (hi > K2m1) hi = K2m1;
-    const int kmax = s < K - 1 ? s : K - 1;
-    const int ny2 = 2 * kmax + 1;
-    const int npair = D == 2 ? (kmax + 1) : (kmax + 1) * ny2;
-
-    // pass 1 (sum) and pass 2 (apply) walk the same modes in the same order
-    for (int phase = 0; phase < 2; ++phase) {
-        double acc[2] = {0, 0};
-        double factor = 0;
-        if (phase == 1) factor = rec[R_FACTOR];
-        if (lo <= hi) {
-            for (int e = threadIdx.x; e < npair; e += NT) {
-                int kx, ky = 0;
-                long long rr;
-                if (D == 2) { kx = e; rr = (long long)kx * kx; }
-                else { kx = e / ny2; ky = e - kx * ny2 - kmax; rr = (long long)kx * kx + (long long)ky * ky; }
-                const long long rlo = lo - rr, rhi = hi - rr;
-                if (rhi < 0) continue;
-                const int a = (int)isqrt_ceil(rlo), b = (int)isqrt_floor(rhi);
-                for (int t = a; t <= b; ++t) {
-                    for (int sg = 0; sg < (t == 0 ? 1 : 2); ++sg) {
-                        const int tt = sg ? -t : t;
-                        const double w = kx == 0 ? 1.0 : 2.0;
-                        size_t o;
-                        int kyv, kzv;
-                        if (D == 2) {
-                            kyv = tt; kzv = 0;
-                            const int kyi = kyv >= 0 ? kyv : kyv + g.KY;
-                            o = ((size_t)kx * g.KY + kyi) * 2;
-                        } else {
-                            kyv = ky; kzv = tt;
-                            const int kyi = kyv >= 0 ? kyv : kyv + g.KY;
-                            const int kzi = kzv >= 0 ? kzv : kzv + g.KZ;
-                            o = ((size_t)kx * g.KY + kyi) * g.KZ + kzi;
-                        }
-                        double2 f[3];
-                        const size_t cst = D == 2 ? 1 : (size_t)g.ps;
-                        if (rnd) {
-                            const double phi = band_phase(kx, kyv, kzv, ctr);
-                            const double kk = sqrt((double)(rr + (long long)tt * tt));
-                            const double kv[3] = {(double)kx, (double)kyv, (double)kzv};
-                            const double2 e = make_double2(sin(phi), cos(phi));
-                            for (int c = 0; c < D; ++c) f[c] = make_double2(kv[c] / kk * e.x, kv[c] / kk * e.y);
-                        } else {
-                            for (int c = 0; c < D; ++c) f[c] = U0[o + c * cst];
-                        }
-                        if (!rnd && D == 2 && project2d) {
-                            // solution.F90:498-501
-                            const double kk = sqrt((double)(rr + (long long)tt * tt));
-                            const double k1 = kx, k2 = kyv;
-                            double2 ud;
-                            ud.x = f[0].x * k1 / kk + f[1].x * k2 / kk;
-                            ud.y = f[0].y * k1 / kk + f[1].y * k2 / kk;
-                            f[0] = make_double2(ud.x * k1 / kk, ud.y * k1 / kk);
-                            f[1] = make_double2(ud.x * k2 / kk, ud.y * k2 / kk);
-                        }
-                        if (phase == 0) {
-                            double e2 = 0, fu = 0;
-                            for (int c = 0; c < D; ++c) {
-                                e2 += f[c].x * f[c].x + f[c].y * f[c].y;
-                                if (rnd) {
-                                    const double2 u = U0[o + c * cst];
-                                    fu += f[c].x * u.x + f[c].y * u.y;   // Re(f conj(u))
-                                }
-                            }
-                            acc[0] += w * e2;
-                            acc[1] += w * fu;
-                        } else {
-                            for (int c = 0; c < D; ++c) {
-                                double2 u = U0[o + c * cst];
-                                U0[o + c * cst] = make_double2(u.x + factor * f[c].x, u.y + factor * f[c].y);
-                            }
-                        }
-                    }
-                }
+    const size_t cst = D == 2 ? 1 : (size_t)g.ps;
+    // entries of the band: list entries, or the k = 0 mode (index -1) for forcek = 0
+    const int nband = forcek == 0 ? 1 : band_hi - band_lo;
+    // the force of list entry j at its state offset o, and the mode's Hermitian weight
+    auto force_of = [&](int j, size_t& o, double& w, double2 (&f)[3]) {
+        int kx = 0, kyv = 0, kzv = 0;
+        if (forcek != 0) {
+            const int idx = modes[band_lo + j];   // ((kx KY + kyi) KZ + kzi)
+            const int kzi = D == 3 ? idx % g.KZ : 0;
+            const int r = D == 3 ? idx / g.KZ : idx;
+            kx = r / g.KY;
+            const int kyi = r - kx * g.KY;
+            kyv = trunc_k(kyi, g.K, g.KY);
+            kzv = D == 3 ? trunc_k(kzi, g.K, g.KZ) : 0;
+            o = D == 2 ? (size_t)idx * 2 : (size_t)idx;
+        } else {
+            o = 0;
+        }
+        w = kx == 0 ? 1.0 : 2.0;
+        const long long m2 = (long long)kx * kx + (long long)kyv * kyv + (long long)kzv * kzv;
+        if (rnd) {
+            const double phi = band_phase(kx, kyv, kzv, ctr);
+            const double kk = sqrt((double)m2);
+            const double kv[3] = {(double)kx, (double)kyv, (double)kzv};
+            const double2 e = make_double2(sin(phi), cos(phi));
+            for (int c = 0; c < D; ++c) f[c] = make_double2(kv[c] / kk * e.x, kv[c] / kk * e.y);
+        } else {
+            for (int c = 0; c < D; ++c) f[c] = U0[o + c * cst];
+        }
+        if (!rnd && D == 2 && project2d) {
+            // solution.F90:498-501
+            const double kk = sqrt((double)m2);
+            const double k1 = kx, k2 = kyv;
+            double2 ud;
+            ud.x = f[0].x * k1 / kk + f[1].x * k2 / kk;
+            ud.y = f[0].y * k1 / kk + f[1].y * k2 / kk;
+            f[0] = make_double2(ud.x * k1 / kk, ud.y * k1 / kk);
+            f[1] = make_double2(ud.x * k2 / kk, ud.y * k2 / kk);
+        }
+    };
+    // pass 1: E (and Fen), fixed order
+    double acc[2] = {0, 0};
+    for (int j = threadIdx.x; j < nband; j += NT) {
+        size_t o;
+        double w;
+        double2 f[3];
+        force_of(j, o, w, f);
+        double e2 = 0, fu = 0;
+        for (int c = 0; c < D; ++c) {
+            e2 += f[c].x * f[c].x + f[c].y * f[c].y;
+            if (rnd) {
+                const double2 u = U0[o + c * cst];
+                fu += f[c].x * u.x + f[c].y * u.y;   // Re(f conj(u))
             }
         }
-        if (phase == 0) {
-            block_sum<2, NT>(acc, scratch);
-            if (threadIdx.x == 0) {
-                double fac, E;
-                if (method == 2) {
-                    E = acc[0];
-                    fac = sqrt(target / E) - 1.0;
-                } else if (method == 5) {
-                    E = acc[0];
-                    const double energy = rec[R_ENERGY];
-                    fac = target > energy ? sqrt((target - energy) / E + 1.0) - 1.0 : 0.0;
-                } else {
-                    const double fen = acc[0], energy = rec[R_ENERGY];
-                    E = acc[1];
-                    fac = method == 3 ? (sqrt(fmax((target - energy) * fen + E * E, 0.0)) - E) / fen : target;
-                    rec[R_FEN] = fen;
-                    *rng = ctr + 1;
-                }
-                rec[R_FACTOR] = fac;
-                rec[R_E] = E;
-            }
-            __syncthreads();
+        acc[0] += w * e2;
+        acc[1] += w * fu;
+    }
+    block_sum<2, NT>(acc, scratch);
+    if (threadIdx.x == 0) {
+        double fac, E;
+        if (method == 2) {
+            E = acc[0];
+            fac = sqrt(target / E) - 1.0;
+        } else if (method == 5) {
+            E = acc[0];
+            const double energy = rec[R_ENERGY];
+            fac = target > energy ? sqrt((target - energy) / E + 1.0) - 1.0 : 0.0;
+        } else {
+            const double fen = acc[0], energy = rec[R_ENERGY];
+            E = acc[1];
+            fac = method == 3 ? (sqrt(fmax((target - energy) * fen + E * E, 0.0)) - E) / fen : target;
+            rec[R_FEN] = fen;
+            *rng = ctr + 1;
+        }
+        rec[R_FACTOR] = fac;
+        rec[R_E] = E;
+        s_factor = fac;
+    }
+    __syncthreads();
+    // pass 2: u += factor * f on the same entries (each thread the entries it summed)
+    const double factor = s_factor;
+    for (int j = threadIdx.x; j < nband; j += NT) {
+        size_t o;
+        double w;
+        double2 f[3];
+        force_of(j, o, w, f);
+        for (int c = 0; c < D; ++c) {
+            const double2 u = U0[o + c * cst];
+            U0[o + c * cst] = make_double2(u.x + factor * f[c].x, u.y + factor * f[c].y);
         }
     }
 }

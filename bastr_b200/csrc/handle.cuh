@@ -109,6 +109,7 @@ struct bastr_handle {
     int* sp_shell_item = nullptr; // [nshell + 1]
     double* sp_item_part = nullptr;
     int n_items = 0;
+    int band_lo = 0, band_hi = 0;   // the forcing band's entries in sp_modes (shell forcek)
     // per-launch profiling (bastr_profile): CUDA events around every launch
     bool prof_on = false;
     std::vector<cudaEvent_t> ev_pool;

@@ -60,53 +60,102 @@ __host__ __device__ constexpr int pow2_floor(int n) {
 }
 
 // Fixed-order block reduction of NV doubles (sum) into every thread's v[]; the tree shape
-// depends only on the block size, so results are bitwise reproducible run to run.  Block
-// sizes that are not powers of two first fold their tail onto the leading power of two.
+// depends only on the block size, so results are bitwise reproducible run to run.  Blocks of
+// whole warps reduce within each warp by butterfly shuffles (lanes l and l^m add the same two
+// values, so every lane holds the same bits), then the warps' sums the same way in warp 0: two
+// barriers instead of log2(NT).  Other block sizes use a shared-memory tree, their tail folded
+// onto the leading power of two first.
 template <int NV, int NT>
 __device__ __forceinline__ void block_sum(double* v, double* scratch /* NV*NT doubles */) {
-    constexpr int P2 = pow2_floor(NT);
     const int t = threadIdx.x;
+    if constexpr (NT % 32 == 0 && NT <= 1024) {
+        constexpr int NW = NT / 32;
+        const int lane = t & 31, w = t >> 5;
 #pragma unroll
-    for (int i = 0; i < NV; ++i) scratch[i * NT + t] = v[i];
-    __syncthreads();
-    if constexpr (P2 != NT) {
-        if (t >= P2) {
+        for (int i = 0; i < NV; ++i)
 #pragma unroll
-            for (int i = 0; i < NV; ++i) scratch[i * NT + t - P2] += scratch[i * NT + t];
+            for (int m = 16; m > 0; m >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], m);
+        if (lane == 0) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) scratch[i * NW + w] = v[i];
         }
         __syncthreads();
-    }
+        if (w == 0) {
 #pragma unroll
-    for (int s = P2 / 2; s > 0; s >>= 1) {
-        if (t < s) {
+            for (int i = 0; i < NV; ++i) {
+                double x = lane < NW ? scratch[i * NW + lane] : 0.0;
 #pragma unroll
-            for (int i = 0; i < NV; ++i) scratch[i * NT + t] += scratch[i * NT + t + s];
+                for (int m = 16; m > 0; m >>= 1) x += __shfl_xor_sync(0xffffffffu, x, m);
+                v[i] = x;
+            }
+        }
+        __syncthreads();   // every warp has read its partials: the totals go where they were
+        if (w == 0 && lane == 0) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) scratch[i * NW] = v[i];
         }
         __syncthreads();
-    }
 #pragma unroll
-    for (int i = 0; i < NV; ++i) v[i] = scratch[i * NT];
-    __syncthreads();
+        for (int i = 0; i < NV; ++i) v[i] = scratch[i * NW];
+        __syncthreads();
+    } else {
+        constexpr int P2 = pow2_floor(NT);
+#pragma unroll
+        for (int i = 0; i < NV; ++i) scratch[i * NT + t] = v[i];
+        __syncthreads();
+        if constexpr (P2 != NT) {
+            if (t >= P2) {
+#pragma unroll
+                for (int i = 0; i < NV; ++i) scratch[i * NT + t - P2] += scratch[i * NT + t];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int s = P2 / 2; s > 0; s >>= 1) {
+            if (t < s) {
+#pragma unroll
+                for (int i = 0; i < NV; ++i) scratch[i * NT + t] += scratch[i * NT + t + s];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] = scratch[i * NT];
+        __syncthreads();
+    }
 }
 
 template <int NT>
 __device__ __forceinline__ double block_min(double v, double* scratch) {
-    constexpr int P2 = pow2_floor(NT);
     const int t = threadIdx.x;
-    scratch[t] = v;
-    __syncthreads();
-    if constexpr (P2 != NT) {
-        if (t >= P2) scratch[t - P2] = fmin(scratch[t - P2], scratch[t]);
-        __syncthreads();
-    }
+    if constexpr (NT % 32 == 0 && NT <= 1024) {
+        constexpr int NW = NT / 32;
+        const int lane = t & 31, w = t >> 5;
 #pragma unroll
-    for (int s = P2 / 2; s > 0; s >>= 1) {
-        if (t < s) scratch[t] = fmin(scratch[t], scratch[t + s]);
+        for (int m = 16; m > 0; m >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, m));
+        if (lane == 0) scratch[w] = v;
         __syncthreads();
+        double r = scratch[0];
+#pragma unroll
+        for (int i = 1; i < NW; ++i) r = fmin(r, scratch[i]);
+        __syncthreads();
+        return r;
+    } else {
+        constexpr int P2 = pow2_floor(NT);
+        scratch[t] = v;
+        __syncthreads();
+        if constexpr (P2 != NT) {
+            if (t >= P2) scratch[t - P2] = fmin(scratch[t - P2], scratch[t]);
+            __syncthreads();
+        }
+#pragma unroll
+        for (int s = P2 / 2; s > 0; s >>= 1) {
+            if (t < s) scratch[t] = fmin(scratch[t], scratch[t + s]);
+            __syncthreads();
+        }
+        double r = scratch[0];
+        __syncthreads();
+        return r;
     }
-    double r = scratch[0];
-    __syncthreads();
-    return r;
 }
 
 // Programmatic dependent launch: the kernels of a step are launched with
