@@ -102,6 +102,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     rank = int(os.environ.get("RANK", 0))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > len(args.train_seeds):
+        # the same test on every rank, before any collective: no rank is left waiting
+        raise SystemExit(f"{world} ranks need at least {world} training seeds, got {len(args.train_seeds)}")
     torch.cuda.set_device(local)
     group = None
     if world > 1:
@@ -110,8 +113,6 @@ def main():
         group = dist.group.WORLD
     seeds = shard_seeds(args.train_seeds, rank, world)
     pairs, dns_ms = make_pairs(seeds, args, device=local)
-    if not pairs:
-        raise SystemExit(f"rank {rank}: no training seeds (more ranks than seeds)")
     net = Net(seed=args.net_seed, device=local)
     tau_rms, hist = train_dp(net, pairs, args.iters, args.lr, group)
     t = torch.tensor([dns_ms], dtype=torch.float64, device="cuda")

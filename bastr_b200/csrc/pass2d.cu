@@ -45,8 +45,11 @@ template <typename T> struct EptOf { static constexpr int v = sizeof(T) == 8 ? B
 #ifndef BASTR_EPT_YFWD_F32
 #define BASTR_EPT_YFWD_F32 8
 #endif
+// The inverse y pass (the step's first pass, from the FP64 state) runs best at 8 points per
+// thread since its lines are TMA-staged: 2048^2 FP32 k2d_yinv_rhs_vg 49.6 -> 43.5 us (16: 248
+// registers, 8: 117-128 and twice the threads).
 #ifndef BASTR_EPT_YINV_F32
-#define BASTR_EPT_YINV_F32 16
+#define BASTR_EPT_YINV_F32 8
 #endif
 #ifndef BASTR_MINB_YINV
 #define BASTR_MINB_YINV 0
