@@ -90,7 +90,7 @@ cudaError_t launch_spectra(bastr_handle* h, double* rec, double* shells_out, uns
 }
 
 // The forcing of a step, and the velocity-gradient statistics of the step (when vg) in the same
-// single-block kernel; without forcing they get their own launch.
+// kernel (one block each, side by side); without forcing they get their own launch.
 cudaError_t launch_forcing(bastr_handle* h, double* rec, bool vg) {
     const int m = h->p.forcemethod;
     const double* vgp = vg ? h->vg_part : nullptr;
@@ -104,7 +104,7 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec, bool vg) {
     }
     if (m == 1) {
         ProfScope ps(h, "k_force_linear", (double)h->n_en_blocks * 8);
-        LAUNCH(launch_k(h, k_force_linear<256>, 1, 256, 0, h->en_part, h->n_en_blocks, rec, h->p.target_energy, h->pend,
+        LAUNCH(launch_k(h, k_force_linear<256>, vgn > 0 ? 2 : 1, 256, 0, h->en_part, h->n_en_blocks, rec, h->p.target_energy, h->pend,
                         vgp, vgn, h->g));
         h->scale_pending = true;
         return cudaGetLastError();
@@ -117,10 +117,10 @@ cudaError_t launch_forcing(bastr_handle* h, double* rec, bool vg) {
         const int proj = (m == 5 && h->g.d == 2 && h->p.lprojectd) ? 1 : 0;
         ProfScope ps(h, "k_force_band", 0);
         if (h->g.d == 2)
-            LAUNCH(launch_k(h, k_force_band<2, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
+            LAUNCH(launch_k(h, k_force_band<2, 256>, vgn > 0 ? 2 : 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
                             h->rng, vgp, vgn, (const int*)h->sp_modes, h->band_lo, h->band_hi));
         else
-            LAUNCH(launch_k(h, k_force_band<3, 256>, 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
+            LAUNCH(launch_k(h, k_force_band<3, 256>, vgn > 0 ? 2 : 1, 256, 0, h->u0, h->g, m, h->p.forcek, h->p.target_energy, proj, rec,
                             h->rng, vgp, vgn, (const int*)h->sp_modes, h->band_lo, h->band_hi));
     }
     return cudaGetLastError();

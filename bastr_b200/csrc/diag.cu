@@ -287,8 +287,9 @@ __global__ void __launch_bounds__(NT) k_sum_partials(const double* __restrict__ 
 // fixed order to sum_k w|u^|^2 = mean(|u|^2) (Parseval with the 1/N forward normalisation);
 // factor = sqrt(target / mean(|u|^2/2)).  The scale u *= factor itself is left pending: the
 // next step's spectra kernel (or k_apply_pending) applies it.
-// With vg_nblk > 0 the kernel first finishes the step's velocity-gradient statistics from the x
-// pass's partials (they are read only from the record, so they need no launch of their own).
+// With vg_nblk > 0 the kernel is launched with a second block that finishes the step's
+// velocity-gradient statistics from the x pass's partials beside the forcing (they are read only
+// from the record, so they need no launch of their own).
 template <int NT>
 __global__ void __launch_bounds__(NT) k_force_linear(const double* __restrict__ part, int n,
                                                      double* __restrict__ rec, double target, double2* pend,
@@ -296,9 +297,9 @@ __global__ void __launch_bounds__(NT) k_force_linear(const double* __restrict__ 
     pdl_wait();
     if (halted(g)) return;
     __shared__ double scratch[7 * NT];
-    if (vg_nblk > 0) {
+    if (blockIdx.x == 1) {   // launched with vg_nblk > 0: the statistics in a block of their own
         velgrad_finish<NT>(vg_part, vg_nblk, g, rec, scratch);
-        __syncthreads();
+        return;
     }
     double acc[1] = {0};
     for (int b = threadIdx.x; b < n; b += NT) acc[0] += part[b];
@@ -369,9 +370,9 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
     if (halted(g)) return;
     __shared__ double scratch[7 * NT];
     __shared__ double s_factor;
-    if (vg_nblk > 0) {   // the step's velocity-gradient statistics, as k_force_linear does
+    if (blockIdx.x == 1) {   // the step's velocity-gradient statistics, as k_force_linear does
         velgrad_finish<NT>(vg_part, vg_nblk, g, rec, scratch);
-        __syncthreads();
+        return;
     }
     const bool rnd = method == 3 || method == 4;
     const unsigned long long ctr = rnd ? *rng : 0ull;
