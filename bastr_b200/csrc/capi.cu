@@ -219,6 +219,7 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
         st = cudaMemset(q, 0, bytes ? bytes : 16);
         h->dev_bytes += (int64_t)bytes;
     }
+    if (st == cudaSuccess) st = track_alloc(h, q, bytes ? bytes : 16);
     *ptr = (P*)q;
 }
 
@@ -226,7 +227,7 @@ void free_all(bastr_handle* h) {
     void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->rng, h->closure_buf, h->tr_buf, h->tr_modes, h->hg_part,
                     h->sg_buf, h->sg_tw,
                     h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
-                    h->sp_item_part};
+                    h->sp_item_part, h->chk_table};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     for (auto& t : h->tw) {
@@ -361,12 +362,12 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
         // MB records of FP32 (32 bytes) and FP64 (64 bytes) values; MB holds the FP64 layout always
         const uint64_t dy[3] = {8, KK, NY / 2}, sy32[2] = {32, KK * 32}, sy64[2] = {64, KK * 64};
         const uint32_t by[3] = {8, 1, BY};
-        const bool ok = encode_map(&h->tm[TM_XA4], h->ma, (int)el, 4, d4, s4, ba, swa) &&
-                        encode_map(&h->tm[TM_XA8], h->ma, (int)el, 4, d8, s8, ba, swa) &&
-                        encode_map(&h->tm[TM_XB8], h->ma, (int)el, 4, d8, s8, bb, swb) &&
-                        encode_map(&h->tm[TM_YMB32], h->mb, 4, 3, dy, sy32, by, 0) &&
-                        encode_map(&h->tm[TM_YMB64], h->mb, 8, 3, dy, sy64, by, 64);
-        if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a mixed-field tensor map");
+        const bool ok = encode_map(h, &h->tm[TM_XA4], h->ma, (int)el, 4, d4, s4, ba, swa) &&
+                        encode_map(h, &h->tm[TM_XA8], h->ma, (int)el, 4, d8, s8, ba, swa) &&
+                        encode_map(h, &h->tm[TM_XB8], h->ma, (int)el, 4, d8, s8, bb, swb) &&
+                        encode_map(h, &h->tm[TM_YMB32], h->mb, 4, 3, dy, sy32, by, 0) &&
+                        encode_map(h, &h->tm[TM_YMB64], h->mb, 8, 3, dy, sy64, by, 64);
+        if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a mixed-field tensor map, or it reaches past its buffer");
     } else if (cs == sizeof(float2) && K <= 256 && g.KY <= 256) {
         // TMA tensor maps of the FP32 3D passes (see TensorMapSlot3): MB [z][kx][f][y] for the x
         // pass (4 consecutive y x every field x every kx x 1 z plane, 32-byte swizzle) and
@@ -379,16 +380,16 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
             const uint64_t F = fins[m];
             const uint64_t dm[4] = {2 * NY, F, KK, NZ}, sm[3] = {NY * 8, F * NY * 8, KK * F * NY * 8};
             const uint32_t bx[4] = {8, (uint32_t)F, (uint32_t)KK, 1};
-            ok = ok && encode_map(&h->tm3[m], h->mb, 4, 4, dm, sm, bx, 32);
+            ok = ok && encode_map(h, &h->tm3[m], h->mb, 4, 4, dm, sm, bx, 32);
         }
         const int finy[2] = {6, 10};
         for (int m = 0; m < 2; ++m) {
             const uint64_t F = finy[m];
             const uint64_t dm[4] = {2 * NZ, F, KY, KK}, sm[3] = {NZ * 8, F * NZ * 8, KY * F * NZ * 8};
             const uint32_t bx[4] = {8, (uint32_t)F + 1, (uint32_t)KY, 1};   // one field past MA's: zeros
-            ok = ok && encode_map(&h->tm3[TM_Y3MA6 + m], h->ma, 4, 4, dm, sm, bx, 32);
+            ok = ok && encode_map(h, &h->tm3[TM_Y3MA6 + m], h->ma, 4, 4, dm, sm, bx, 32);
         }
-        if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a 3D mixed-field tensor map");
+        if (!ok) return fail(h, BASTR_E_CUDA, "cuTensorMapEncodeTiled rejected a 3D mixed-field tensor map, or it reaches past its buffer");
     }
 
     const int ns[3] = {g.nx, g.ny, d == 3 ? g.nz : 0};
@@ -400,6 +401,8 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
         h->tw[a].n = ns[a];
         CK(cudaMalloc(&h->tw[a].d64, ns[a] * sizeof(double2)));
         CK(cudaMalloc(&h->tw[a].d32, ns[a] * sizeof(float2)));
+        CK(track_alloc(h, h->tw[a].d64, ns[a] * sizeof(double2)));
+        CK(track_alloc(h, h->tw[a].d32, ns[a] * sizeof(float2)));
         CK(cudaMemcpy(h->tw[a].d64, t64.data(), ns[a] * sizeof(double2), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->tw[a].d32, t32.data(), ns[a] * sizeof(float2), cudaMemcpyHostToDevice));
     }
@@ -640,7 +643,9 @@ int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, dou
     const unsigned int halt = words[0];
     if (words[1] != 0) {
         CK(cudaMemsetAsync(h->done + T_ERR, 0, sizeof(unsigned int), h->stream));
-        return fail(h, BASTR_E_CUDA, "a kernel of the last batch gave up waiting for its TMA staging (error word %u)",
+        return fail(h, BASTR_E_CUDA,
+                    "a kernel of the last batch reported an error (error word %u: 1 = a TMA staging wait gave up, "
+                    "2 = an index check of the checked build failed)",
                     words[1]);
     }
     // the stop word belongs to the last batch (chunk_used steps); a NaN step within the records asked for
@@ -843,10 +848,15 @@ int bastr_transfer(bastr_handle* h, double* T, double* T1, double* T2) {
     const size_t n = (size_t)g.nx * g.ny * g.nz;
     const size_t narr = (size_t)(D + D * D + D + D + D * D);
     const size_t nmodes = (size_t)g.K * g.KY * g.KZ;
-    if (!h->tr_buf) CK(cudaMalloc(&h->tr_buf, narr * n * sizeof(double2)));
-    if (!h->tr_modes)
-        CK(cudaMalloc(&h->tr_modes, (nmodes * 3 + (size_t)std::max(h->n_items, 1) * 3 + 3 * (size_t)h->nshell) *
-                                        sizeof(double)));
+    if (!h->tr_buf) {
+        CK(cudaMalloc(&h->tr_buf, narr * n * sizeof(double2)));
+        CK(track_alloc(h, h->tr_buf, narr * n * sizeof(double2)));
+    }
+    if (!h->tr_modes) {
+        const size_t bytes = (nmodes * 3 + (size_t)std::max(h->n_items, 1) * 3 + 3 * (size_t)h->nshell) * sizeof(double);
+        CK(cudaMalloc(&h->tr_modes, bytes));
+        CK(track_alloc(h, h->tr_modes, bytes));
+    }
     double2* U = h->tr_buf;
     double2* Dv = U + (size_t)D * n;
     double2* tA = Dv + (size_t)D * D * n;
@@ -905,8 +915,14 @@ int bastr_hitgen(bastr_handle* h, int32_t variant, uint64_t seed, double* u1, do
     const size_t n = (size_t)g.nx * g.ny * g.nz;
     const size_t narr = (size_t)(D + D * D + D + D + D * D);   // the transfer buffer's size
     constexpr int NB = 148 * 4, NT = 256;
-    if (!h->tr_buf) CK(cudaMalloc(&h->tr_buf, narr * n * sizeof(double2)));
-    if (!h->hg_part) CK(cudaMalloc(&h->hg_part, (size_t)NB * 4 * sizeof(double)));
+    if (!h->tr_buf) {
+        CK(cudaMalloc(&h->tr_buf, narr * n * sizeof(double2)));
+        CK(track_alloc(h, h->tr_buf, narr * n * sizeof(double2)));
+    }
+    if (!h->hg_part) {
+        CK(cudaMalloc(&h->hg_part, (size_t)NB * 4 * sizeof(double)));
+        CK(track_alloc(h, h->hg_part, (size_t)NB * 4 * sizeof(double)));
+    }
     const bool bis = variant == 1;
     double2* R = h->tr_buf;
     double2* A = R + n;
@@ -994,6 +1010,8 @@ int bastr_subgrid(bastr_handle* h, int32_t r, float* d_ubar, float* d_tau) {
         h->sg_r = 0;
         CK(cudaMalloc(&h->sg_buf, (3 * N + nc * (4 * (size_t)D + 3)) * sizeof(double)));
         CK(cudaMalloc(&h->sg_tw, (size_t)(cns[0] + cns[1] + cns[2]) * sizeof(double2)));
+        CK(track_alloc(h, h->sg_buf, (3 * N + nc * (4 * (size_t)D + 3)) * sizeof(double)));
+        CK(track_alloc(h, h->sg_tw, (size_t)(cns[0] + cns[1] + cns[2]) * sizeof(double2)));
         size_t o = 0;
         for (int a = 0; a < 3; ++a) {
             std::vector<double2> t64;
@@ -1066,7 +1084,10 @@ int bastr_closure_apply(bastr_handle* h, const uint16_t* d_w, float scale, doubl
     CK(cudaSetDevice(h->device));
     const size_t n = (size_t)h->g.nx * h->g.ny * h->g.nz;
     if (3 * n >= ((size_t)1 << 31)) return fail(h, BASTR_E_UNSUPPORTED, "closure network: grid too large");
-    if (!h->closure_buf) CK(cudaMalloc(&h->closure_buf, 3 * n * sizeof(float)));
+    if (!h->closure_buf) {
+        CK(cudaMalloc(&h->closure_buf, 3 * n * sizeof(float)));
+        CK(track_alloc(h, h->closure_buf, 3 * n * sizeof(float)));
+    }
     CK(flush_pending_scale(h));
     CK(to_physical(h));
     const int grid = (int)std::min<size_t>((n + kFwdNT - 1) / kFwdNT, 148 * 4);

@@ -60,12 +60,12 @@ __device__ __forceinline__ void spectra_mode(double2* __restrict__ U0, const Geo
     double es, ed;
     if constexpr (D == 2) {
         const size_t o = ((size_t)kx * g.KY + kyi) * 2;
-        double2 a = U0[o], b = U0[o + 1];
+        double2 a = BASTR_AT(U0, o, g), b = BASTR_AT(U0, o + 1, g);
         if (scale) {   // the linear forcing of the previous step, applied here (forcing3D-style u *= f)
             a = make_double2(f * a.x, f * a.y);
             b = make_double2(f * b.x, f * b.y);
-            U0[o] = a;
-            U0[o + 1] = b;
+            BASTR_AT(U0, o, g) = a;
+            BASTR_AT(U0, o + 1, g) = b;
         }
         // usspe = u1 k2/kk - u2 k1/kk ; udspe = u1 k1/kk + u2 k2/kk  (solution.F90:958-959)
         const double usx = a.x * h2 - b.x * h1, usy = a.y * h2 - b.y * h1;
@@ -76,14 +76,14 @@ __device__ __forceinline__ void spectra_mode(double2* __restrict__ U0, const Geo
     } else {
         const int kzi = kz >= 0 ? kz : kz + g.KZ;
         const size_t o = ((size_t)kx * g.KY + kyi) * g.KZ + kzi;
-        double2 a = U0[o], b = U0[o + g.ps], c = U0[o + 2 * g.ps];
+        double2 a = BASTR_AT(U0, o, g), b = BASTR_AT(U0, o + g.ps, g), c = BASTR_AT(U0, o + 2 * g.ps, g);
         if (scale) {   // the linear forcing of the previous step, applied here (solution.F90:328-331)
             a = make_double2(f * a.x, f * a.y);
             b = make_double2(f * b.x, f * b.y);
             c = make_double2(f * c.x, f * c.y);
-            U0[o] = a;
-            U0[o + g.ps] = b;
-            U0[o + 2 * g.ps] = c;
+            BASTR_AT(U0, o, g) = a;
+            BASTR_AT(U0, o + g.ps, g) = b;
+            BASTR_AT(U0, o + 2 * g.ps, g) = c;
         }
         // solution.F90:1047-1053
         const double udx = a.x * h1 + b.x * h2 + c.x * h3;
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
             const double2 e = make_double2(sin(phi), cos(phi));
             for (int c = 0; c < D; ++c) f[c] = make_double2(kv[c] / kk * e.x, kv[c] / kk * e.y);
         } else {
-            for (int c = 0; c < D; ++c) f[c] = U0[o + c * cst];
+            for (int c = 0; c < D; ++c) f[c] = BASTR_AT(U0, o + c * cst, g);
         }
         if (!rnd && D == 2 && project2d) {
             // solution.F90:498-501
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
         for (int c = 0; c < D; ++c) {
             e2 += f[c].x * f[c].x + f[c].y * f[c].y;
             if (rnd) {
-                const double2 u = U0[o + c * cst];
+                const double2 u = BASTR_AT(U0, o + c * cst, g);
                 fu += f[c].x * u.x + f[c].y * u.y;   // Re(f conj(u))
             }
         }
@@ -464,8 +464,8 @@ __global__ void __launch_bounds__(NT) k_force_band(double2* __restrict__ U0, Geo
         double2 f[3];
         force_of(j, o, w, f);
         for (int c = 0; c < D; ++c) {
-            const double2 u = U0[o + c * cst];
-            U0[o + c * cst] = make_double2(u.x + factor * f[c].x, u.y + factor * f[c].y);
+            const double2 u = BASTR_AT(U0, o + c * cst, g);
+            BASTR_AT(U0, o + c * cst, g) = make_double2(u.x + factor * f[c].x, u.y + factor * f[c].y);
         }
     }
 }

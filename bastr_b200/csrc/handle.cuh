@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -121,6 +122,10 @@ struct bastr_handle {
     // TMA tensor maps of the mixed-field buffers (2D, compute precision), built at creation
     CUtensorMap tm[5] = {};
     CUtensorMap tm3[4] = {};
+    // the handle's device buffers as [begin, end) byte ranges: every tensor map is checked to lie
+    // inside one at creation, and the index-checking build copies them to chk_table (Geo::chk)
+    std::vector<std::pair<uint64_t, uint64_t>> ranges;
+    CheckTable* chk_table = nullptr;
 };
 
 namespace bastr_impl {
@@ -158,11 +163,50 @@ inline EncodeTiledFn encode_tiled_fn() {
     return fn;
 }
 
+// Records a device buffer of the handle (see bastr_handle::ranges); with the index-checking
+// build the device copy of the table is refreshed, so a buffer allocated after creation is
+// known to the checked kernels too.  Not for use while a stream is being captured.
+inline cudaError_t track_alloc(bastr_handle* h, const void* p, size_t bytes) {
+    if (!p) return cudaSuccess;
+    h->ranges.push_back({(uint64_t)p, (uint64_t)p + bytes});
+#ifdef BASTR_CHECKED
+    if (!h->chk_table) {
+        const cudaError_t e = cudaMalloc(&h->chk_table, sizeof(CheckTable));
+        if (e != cudaSuccess) return e;
+        h->g.chk = h->chk_table;
+    }
+    // BASTR_CHECK_SHRINK=n (tests of the checker itself): each registered range loses its last n
+    // bytes, so in-bounds accesses near a buffer's end are reported (and go to the scratch line)
+    // although no access leaves its buffer
+    static const uint64_t shrink = [] {
+        const char* v = std::getenv("BASTR_CHECK_SHRINK");
+        return v ? (uint64_t)std::strtoull(v, nullptr, 10) : 0ull;
+    }();
+    CheckTable t{};
+    t.n = (int)std::min<size_t>(h->ranges.size(), kCheckRanges);
+    for (int i = 0; i < t.n; ++i) {
+        t.lo[i] = h->ranges[i].first;
+        t.hi[i] = std::max(h->ranges[i].first, h->ranges[i].second - std::min(shrink, h->ranges[i].second));
+    }
+    return cudaMemcpy(h->chk_table, &t, sizeof t, cudaMemcpyHostToDevice);
+#else
+    return cudaSuccess;
+#endif
+}
+
 // A tiled tensor map of `rank` dimensions over a buffer of this GPU (dims innermost first, in
 // elements of `elem` bytes; strides of dims 1.. in bytes); swizzle in bytes (0, 32, 64, 128).
-// Out-of-range box elements read as zero.  Returns false when the driver rejects it.
-inline bool encode_map(CUtensorMap* m, const void* base, int elem, int rank, const uint64_t* dims,
-                       const uint64_t* strides, const uint32_t* box, int swizzle) {
+// Out-of-range box elements read as zero.  Returns false when the driver rejects it, or when
+// the map's extent (the last element's byte offset plus its size) reaches past the handle's
+// buffer that holds `base`: the copy engine would read outside the allocation.
+inline bool encode_map(const bastr_handle* h, CUtensorMap* m, const void* base, int elem, int rank,
+                       const uint64_t* dims, const uint64_t* strides, const uint32_t* box, int swizzle) {
+    uint64_t extent = (dims[0] - 1) * (uint64_t)elem + (uint64_t)elem;
+    for (int i = 1; i < rank; ++i) extent += (dims[i] - 1) * strides[i - 1];
+    const uint64_t a = (uint64_t)base;
+    bool inside = false;
+    for (const auto& r : h->ranges) inside = inside || (a >= r.first && a + extent <= r.second);
+    if (!inside) return false;
     EncodeTiledFn fn = encode_tiled_fn();
     if (!fn) return false;
     cuuint64_t gd[5], gs[4];

@@ -175,7 +175,7 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
                 bulk_load(stg, S + (size_t)kx0 * KY * 2, (uint32_t)colbytes, &bar);
             }
         } else {
-            stage_line(stg, S + (size_t)kx0 * KY * 2, ncol * colbytes);
+            stage_line(stg, S + (size_t)kx0 * KY * 2, ncol * colbytes, g);
             cp_async_commit();
         }
     };
@@ -241,7 +241,8 @@ k2d_yinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
 #pragma unroll
                 for (int e = 0; e < EPT; ++e) {
                     const int y = FFT::out_pos(t, e);
-                    st2<T>(dst + (size_t)y * W, v[e], grp * UG + 1 < F ? v[EPT + e] : mk<T>(0, 0));
+                    st2<T>(BASTR_CHK(dst + (size_t)y * W, 2 * sizeof(cplx<T>), g), v[e],
+                           grp * UG + 1 < F ? v[EPT + e] : mk<T>(0, 0));
                 }
             }
         }
@@ -386,8 +387,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
             return;
         } else if constexpr (MODE == XM_FROM_PHYS) {
             double* d = reinterpret_cast<double*>(stg);
-            stage_line(d, phys_in + (size_t)y0 * NX, nrow * NX * 8);
-            stage_line(d + G * NX, phys_in + (size_t)NY * NX + (size_t)y0 * NX, nrow * NX * 8);
+            stage_line(d, phys_in + (size_t)y0 * NX, nrow * NX * 8, g);
+            stage_line(d + G * NX, phys_in + (size_t)NY * NX + (size_t)y0 * NX, nrow * NX * 8, g);
         } else {
             // rows y0.. of every (kx, pair) -> staging [kx][pair][row][W], KSTR elements per kx
             constexpr int W = FIN < 4 ? FIN : 4;
@@ -400,7 +401,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 // chunks holding only fields past FLIVE are never read
                 if (r < nrow && pr * W + c * (16 / (int)sizeof(cplx<T>)) < P::FLIVE) {
                     cp_async16(stg + (size_t)k * P::KSTR * sizeof(cplx<T>) + (size_t)((pr * G + r) * C16 + c) * 16,
-                               MA + (((size_t)k * (ftot / W) + pr) * NY + y0 + r) * W + c * (16 / (int)sizeof(cplx<T>)));
+                               BASTR_CHK(MA + (((size_t)k * (ftot / W) + pr) * NY + y0 + r) * W +
+                                             c * (16 / (int)sizeof(cplx<T>)), 16, g));
                 }
             }
         }
@@ -518,8 +520,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 for (int e = 0; e < EPT; ++e) {
                     const int x = IFFT::out_pos(t, e);
                     const size_t o = (size_t)y * NX + x;
-                    phys_out[o] = (double)v[e].x;
-                    phys_out[(size_t)NY * NX + o] = (double)v[e].y;
+                    BASTR_AT(phys_out, o, g) = (double)v[e].x;
+                    BASTR_AT(phys_out, (size_t)NY * NX + o, g) = (double)v[e].y;
                 }
             }
         } else {
@@ -575,8 +577,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
                 for (int k = t; k < K; k += NTR) {
                     const cplx<T> Z = sm[pidx(k)];
                     const cplx<T> Zc = cconj<T>(sm[pidx(k == 0 ? 0 : NX - k)]);
-                    st2<T>(MB + (((size_t)(y >> 1) * K + k) * 2 + (y & 1)) * 2, cscale<T>(cadd<T>(Z, Zc), (T)0.5),
-                           cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5));
+                    st2<T>(BASTR_CHK(MB + (((size_t)(y >> 1) * K + k) * 2 + (y & 1)) * 2, 2 * sizeof(cplx<T>), g),
+                           cscale<T>(cadd<T>(Z, Zc), (T)0.5), cscale<T>(cmulni<T>(csub<T>(Z, Zc)), (T)0.5));
                 }
             }
         }
@@ -593,8 +595,8 @@ k2d_xpass(const cplx<T>* __restrict__ MA, int ftot, cplx<T>* __restrict__ MB,
         const double dm = -block_min<NT>(-divmax, scratch);
         if (threadIdx.x == 0) {
 #pragma unroll
-            for (int i = 0; i < 7; ++i) vg_part[(size_t)blockIdx.x * 8 + i] = acc[i];
-            vg_part[(size_t)blockIdx.x * 8 + 7] = dm;
+            for (int i = 0; i < 7; ++i) BASTR_AT(vg_part, (size_t)blockIdx.x * 8 + i, g) = acc[i];
+            BASTR_AT(vg_part, (size_t)blockIdx.x * 8 + 7, g) = dm;
         }
     }
 }
@@ -726,7 +728,8 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
             const int col = q % G, y = q / G;
             if (col < ncol)
                 cp_async16(reinterpret_cast<unsigned char*>(stg) + ((size_t)(col * NY + y) * 2 * sizeof(cplx<T>) + c * 16),
-                           MB + (((size_t)(y >> 1) * K + kx0 + col) * 2 + (y & 1)) * 2 + c * (16 / (int)sizeof(cplx<T>)));
+                           BASTR_CHK(MB + (((size_t)(y >> 1) * K + kx0 + col) * 2 + (y & 1)) * 2 +
+                                         c * (16 / (int)sizeof(cplx<T>)), 16, g));
         }
         cp_async_commit();
     };
@@ -807,7 +810,7 @@ k2d_yfwd(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo g,
             double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
             double r[1] = {en};
             block_sum<1, NT>(r, scratch);
-            if (threadIdx.x == 0) io.energy_part[blockIdx.x] = r[0];
+            if (threadIdx.x == 0) BASTR_AT(io.energy_part, blockIdx.x, io) = r[0];
         }
     }
 }
@@ -895,7 +898,8 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
             const int col = q % G, y = q / G;
             if (col < ncol)
                 cp_async16(reinterpret_cast<unsigned char*>(stg) + ((size_t)(col * NY + y) * 2 * sizeof(cplx<T>) + c * 16),
-                           MB + (((size_t)(y >> 1) * K + kx0 + col) * 2 + (y & 1)) * 2 + c * (16 / (int)sizeof(cplx<T>)));
+                           BASTR_CHK(MB + (((size_t)(y >> 1) * K + kx0 + col) * 2 + (y & 1)) * 2 +
+                                         c * (16 / (int)sizeof(cplx<T>)), 16, g));
         }
         cp_async_commit();
     };
@@ -987,7 +991,8 @@ k2d_yfwd_inv(const cplx<T>* __restrict__ MB, StageIO<T> io, int input_is_u0, Geo
             if (valid) {
                 cplx<T>* dst = MA + (size_t)kx * (FTOT / W) * NY * W + 2 * c;
 #pragma unroll
-                for (int e = 0; e < EPT; ++e) st2<T>(dst + (size_t)IFFT::out_pos(t, e) * W, u[e], u[EPT + e]);
+                for (int e = 0; e < EPT; ++e)
+                    st2<T>(BASTR_CHK(dst + (size_t)IFFT::out_pos(t, e) * W, 2 * sizeof(cplx<T>), g), u[e], u[EPT + e]);
             }
         }
     }

@@ -83,7 +83,7 @@ k3d_zinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
         const int nl = min(G, nlines - l0);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-            stage_line(stg + c * pe, S + c * g.ps + (size_t)l0 * KZ, nl * KZ * (int)sizeof(cplx<TIN>));
+            stage_line(stg + c * pe, S + c * g.ps + (size_t)l0 * KZ, nl * KZ * (int)sizeof(cplx<TIN>), g);
         cp_async_commit();
     };
     int item = blockIdx.x;
@@ -142,7 +142,7 @@ k3d_zinv(const cplx<TIN>* __restrict__ S, cplx<T>* __restrict__ MA, int ftot, Ge
                 for (int u = 0; u < UG; ++u) {
                     if (grp * UG + u < F) {
 #pragma unroll
-                        for (int e = 0; e < EPT; ++e) dst[(size_t)u * NZ + FFT::out_pos(t, e)] = v[u * EPT + e];
+                        for (int e = 0; e < EPT; ++e) BASTR_AT(dst, (size_t)u * NZ + FFT::out_pos(t, e), g) = v[u * EPT + e];
                     }
                 }
             }
@@ -238,8 +238,8 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
         for (int i = threadIdx.x; i < total; i += P::NT) {
             const int kf = i / NCH, c = i - kf * NCH;
             const char* sp = src + (size_t)kf * NZ * sizeof(cplx<T>) + c * CH;
-            if constexpr (CH == 16) cp_async16(d + (size_t)kf * RB + c * CH, sp);
-            else cp_async8(d + (size_t)kf * RB + c * CH, sp);
+            if constexpr (CH == 16) cp_async16(d + (size_t)kf * RB + c * CH, BASTR_CHK(sp, 16, g));
+            else cp_async8(d + (size_t)kf * RB + c * CH, BASTR_CHK(sp, 8, g));
         }
         cp_async_commit();
     };
@@ -312,7 +312,7 @@ k3d_yinv(const cplx<T>* __restrict__ MA, cplx<T>* __restrict__ MB, Geo g, const 
                 for (int u = 0; u < UG; ++u) {
                     if (grp * UG + u < F) {
 #pragma unroll
-                        for (int e = 0; e < EPT; ++e) dst[(size_t)u * NY + FFT::out_pos(t, e)] = v[u * EPT + e];
+                        for (int e = 0; e < EPT; ++e) BASTR_AT(dst, (size_t)u * NY + FFT::out_pos(t, e), g) = v[u * EPT + e];
                     }
                 }
             }
@@ -442,7 +442,7 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
         } else if constexpr (MODE == X3_FROM_PHYS) {
             double* d = reinterpret_cast<double*>(stg);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) stage_line(d + (size_t)c * G * NX, phys_in + c * npts + (size_t)r0 * NX, G * NX * 8);
+            for (int c = 0; c < 3; ++c) stage_line(d + (size_t)c * G * NX, phys_in + c * npts + (size_t)r0 * NX, G * NX * 8, g);
         } else {
             // gather [kx][f][row] from MB[z][kx][f][y]: G consecutive y per (kx, f)
             const int z0 = r0 / NY, y0 = r0 - z0 * NY;
@@ -457,8 +457,8 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
                 const int k = kf / FIN;
                 const char* sp = src + ((size_t)kf * NY * sizeof(cplx<T>)) + c * CH;
                 char* dp = d + (size_t)k * P::KSTR * sizeof(cplx<T>) + (size_t)(kf - k * FIN) * RB + c * CH;
-                if constexpr (CH == 16) cp_async16(dp, sp);
-                else cp_async8(dp, sp);
+                if constexpr (CH == 16) cp_async16(dp, BASTR_CHK(sp, 16, g));
+                else cp_async8(dp, BASTR_CHK(sp, 8, g));
             }
         }
         cp_async_commit();
@@ -547,9 +547,9 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
                 for (int e = 0; e < EPT; ++e) {
                     const int x = IFFT::out_pos(t, e);
                     const size_t o = (size_t)row * NX + x;
-                    phys_out[o] = (double)v[e].x;
-                    phys_out[npts + o] = (double)v[e].y;
-                    phys_out[2 * npts + o] = (double)v[EPT + e].x;
+                    BASTR_AT(phys_out, o, g) = (double)v[e].x;
+                    BASTR_AT(phys_out, npts + o, g) = (double)v[e].y;
+                    BASTR_AT(phys_out, 2 * npts + o, g) = (double)v[EPT + e].x;
                 }
             }
         } else {
@@ -616,7 +616,7 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
             const int r0 = item * G, z0 = r0 / NY, y0 = r0 - z0 * NY;
             for (int i = threadIdx.x; i < K * G * 3; i += NT) {
                 const int k = i / (G * 3), rem = i - k * (G * 3);
-                MC[(((size_t)z0 * K + k) * NY + y0) * 3 + rem] = tile[(size_t)k * P::TSTR + rem];
+                BASTR_AT(MC, (((size_t)z0 * K + k) * NY + y0) * 3 + rem, g) = tile[(size_t)k * P::TSTR + rem];
             }
         }
     }
@@ -632,8 +632,8 @@ k3d_xpass(const cplx<T>* __restrict__ MB, cplx<T>* __restrict__ MC, const double
         const double dm = -block_min<NT>(-divmax, scratch);
         if (threadIdx.x == 0) {
 #pragma unroll
-            for (int i = 0; i < 7; ++i) vg_part[(size_t)blockIdx.x * 8 + i] = acc[i];
-            vg_part[(size_t)blockIdx.x * 8 + 7] = dm;
+            for (int i = 0; i < 7; ++i) BASTR_AT(vg_part, (size_t)blockIdx.x * 8 + i, g) = acc[i];
+            BASTR_AT(vg_part, (size_t)blockIdx.x * 8 + 7, g) = dm;
         }
     }
 }
@@ -678,7 +678,7 @@ k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const 
         const int nl = min(G, nlines - l0);
         for (int j = 0; j < nl; ++j) {
             const int l = l0 + j, kx = l / NZ, z = l - kx * NZ;
-            stage_line(stg + (size_t)j * NY * 3, MC + ((size_t)z * K + kx) * NY * 3, NY * 3 * (int)sizeof(cplx<T>));
+            stage_line(stg + (size_t)j * NY * 3, MC + ((size_t)z * K + kx) * NY * 3, NY * 3 * (int)sizeof(cplx<T>), g);
         }
         cp_async_commit();
     };
@@ -715,7 +715,7 @@ k3d_yfwd(const cplx<T>* __restrict__ MC, cplx<T>* __restrict__ MD, Geo g, const 
             const int l0 = item * G, kx0 = l0 / NZ, z0 = l0 - kx0 * NZ;
             for (int i = threadIdx.x; i < KY * G * 3; i += P::NT) {
                 const int kyi = i / (G * 3), rem = i - kyi * (G * 3);
-                MD[(((size_t)kx0 * KY + kyi) * NZ + z0) * 3 + rem] = tile[(size_t)kyi * P::TS + rem];
+                BASTR_AT(MD, (((size_t)kx0 * KY + kyi) * NZ + z0) * 3 + rem, g) = tile[(size_t)kyi * P::TS + rem];
             }
         }
     }
@@ -753,7 +753,7 @@ k3d_zfwd(const cplx<T>* __restrict__ MD, StageIO<T> io, int input_is_u0, Geo g, 
     const int nitems = (nlines + G - 1) / G;
     auto issue = [&](int item) {
         const int l0 = item * G;
-        stage_line(stg, MD + (size_t)l0 * NZ * 3, min(G, nlines - l0) * NZ * 3 * (int)sizeof(cplx<T>));
+        stage_line(stg, MD + (size_t)l0 * NZ * 3, min(G, nlines - l0) * NZ * 3 * (int)sizeof(cplx<T>), g);
         cp_async_commit();
     };
     const double inv_n = g.inv_n;
@@ -821,7 +821,7 @@ k3d_zfwd(const cplx<T>* __restrict__ MD, StageIO<T> io, int input_is_u0, Geo g, 
             double* scratch = reinterpret_cast<double*>(smraw + P::STAGE);
             double r[1] = {en};
             block_sum<1, NT>(r, scratch);
-            if (threadIdx.x == 0) io.energy_part[blockIdx.x] = r[0];
+            if (threadIdx.x == 0) BASTR_AT(io.energy_part, blockIdx.x, io) = r[0];
         }
     }
 }

@@ -15,6 +15,22 @@
 
 namespace bastr {
 
+// ---------------------------------------------------------------------------------------------
+// Index-checking build (-DBASTR_CHECKED): the library's own memory checker.  A handle registers
+// every device buffer it allocates in a CheckTable in device memory (Geo::chk); the checked
+// accesses (the passes' staging copies and output stores, the stage epilogue's state reads and
+// writes, the spectra and forcing gathers) verify that their bytes lie inside one registered
+// buffer.  An access that does not sets ERR_INDEX in the handle's error word and goes to a
+// scratch line instead, so the kernel runs on and the batch reports BASTR_E_CUDA.  In the normal
+// build the checks compile to nothing and Geo::chk is null.
+// ---------------------------------------------------------------------------------------------
+constexpr int kCheckRanges = 64;
+struct CheckTable {
+    int n;
+    unsigned long long lo[kCheckRanges], hi[kCheckRanges];   // [lo, hi) byte ranges
+};
+constexpr unsigned int ERR_INDEX = 2u;   // error-word bit (bit 1 is a TMA wait that gave up)
+
 struct Geo {
     int nx, ny, nz;     // grid (nz == 1 in 2D)
     int d;              // 2 or 3
@@ -32,7 +48,29 @@ struct Geo {
     // Error word of the handle (never null in a handle's launches): kernels record failures
     // there (e.g. a TMA completion wait that gave up), and the host reports them after the batch.
     unsigned int* err;
+    const CheckTable* chk;   // the handle's buffers (index-checking build), else null
 };
+
+#ifdef BASTR_CHECKED
+static __device__ __align__(16) unsigned char g_check_scratch[64];
+// p if [p, p + bytes) lies inside one buffer of the table (or there is no table), else records
+// ERR_INDEX and returns the scratch line (at most 64 bytes are accessed through it).
+template <typename P>
+__device__ __forceinline__ P* checked_ptr(P* p, size_t bytes, const CheckTable* t, unsigned int* err) {
+    if (!t) return p;
+    const unsigned long long a = reinterpret_cast<unsigned long long>(p), b = a + bytes;
+    for (int i = 0; i < t->n; ++i)
+        if (a >= t->lo[i] && b <= t->hi[i]) return p;
+    if (err) atomicOr(err, ERR_INDEX);
+    return reinterpret_cast<P*>(g_check_scratch);
+}
+// the checked address of an access of `bytes` bytes at p; c: anything with .chk and .err
+#define BASTR_CHK(p, bytes, c) ::bastr::checked_ptr((p), (size_t)(bytes), (c).chk, (c).err)
+#else
+#define BASTR_CHK(p, bytes, c) (p)
+#endif
+// element i of array a, checked
+#define BASTR_AT(a, i, c) (*BASTR_CHK(&(a)[i], sizeof((a)[0]), c))
 
 // True when an earlier kernel of the batch found a NaN energy; the same for every thread of the
 // grid (the word is written by a kernel that completed before this one's pdl_wait returned).
@@ -200,6 +238,8 @@ struct StageIO {
     cplx<T>* us;         // stage input of the next evaluation
     cplx<T>* acc;        // RK accumulator k1 + 4 k2
     double* energy_part; // per-block sum of w*|u0_new|^2 (RK3 / CN_LAST), or null
+    const CheckTable* chk;   // Geo::chk and Geo::err, for the checked accesses
+    unsigned int* err;
 };
 
 __device__ __forceinline__ double2 dscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
@@ -219,10 +259,10 @@ __device__ __forceinline__ void epi_load(EpiIn<T, D>& in, size_t o, size_t cst, 
     if constexpr (EPI != EPI_STORE) {
 #pragma unroll
         for (int c = 0; c < D; ++c) {
-            in.a[c] = io.u0[o + c * cst];
+            in.a[c] = BASTR_AT(io.u0, o + c * cst, io);
             // RK2 re-forms its stage input u0 + dt/2 k1 from a and p instead of reading it
-            if (!from_u0 && EPI != EPI_RK2) in.s[c] = io.us[o + c * cst];
-            if constexpr (EPI == EPI_RK2 || EPI == EPI_RK3) in.p[c] = io.acc[o + c * cst];
+            if (!from_u0 && EPI != EPI_RK2) in.s[c] = BASTR_AT(io.us, o + c * cst, io);
+            if constexpr (EPI == EPI_RK2 || EPI == EPI_RK3) in.p[c] = BASTR_AT(io.acc, o + c * cst, io);
         }
     }
 }
@@ -241,7 +281,7 @@ __device__ __forceinline__ void rk_apply(double2* v, const double* k, double m2,
                                          const Geo& g, double w, double& en, cplx<T>* next = nullptr) {
     if constexpr (EPI == EPI_STORE) {
 #pragma unroll
-        for (int c = 0; c < D; ++c) io.u0[o + c * cst] = v[c];
+        for (int c = 0; c < D; ++c) BASTR_AT(io.u0, o + c * cst, io) = v[c];
         return;
     } else {
         const double nu = g.nu, dt = g.dt;
@@ -284,30 +324,30 @@ __device__ __forceinline__ void rk_apply(double2* v, const double* k, double m2,
         for (int c = 0; c < D; ++c) {
             const double2 a = in.a[c];
             if constexpr (EPI == EPI_RK1) {
-                io.acc[o + c * cst] = cvt<double2, cplx<T>>(v[c]);
+                BASTR_AT(io.acc, o + c * cst, io) = cvt<double2, cplx<T>>(v[c]);
                 const cplx<T> u = cvt<double2, cplx<T>>(make_double2(a.x + dt * v[c].x / 2.0, a.y + dt * v[c].y / 2.0));
-                if constexpr (STORE_US) io.us[o + c * cst] = u;
+                if constexpr (STORE_US) BASTR_AT(io.us, o + c * cst, io) = u;
                 if constexpr (NEXT) next[c] = u;
             } else if constexpr (EPI == EPI_RK2) {
                 const double2 p = cvt<cplx<T>, double2>(in.p[c]);
                 const cplx<T> u = cvt<double2, cplx<T>>(
                     make_double2(a.x - dt * p.x + dt2 * v[c].x, a.y - dt * p.y + dt2 * v[c].y));
-                io.us[o + c * cst] = u;
+                BASTR_AT(io.us, o + c * cst, io) = u;
                 if constexpr (NEXT) next[c] = u;
-                io.acc[o + c * cst] = cvt<double2, cplx<T>>(make_double2(p.x + 4.0 * v[c].x, p.y + 4.0 * v[c].y));
+                BASTR_AT(io.acc, o + c * cst, io) = cvt<double2, cplx<T>>(make_double2(p.x + 4.0 * v[c].x, p.y + 4.0 * v[c].y));
             } else if constexpr (EPI == EPI_RK3) {
                 const double2 p = cvt<cplx<T>, double2>(in.p[c]);
                 const double2 n = make_double2(a.x + dt * (p.x + v[c].x) / 6.0, a.y + dt * (p.y + v[c].y) / 6.0);
-                io.u0[o + c * cst] = n;
+                BASTR_AT(io.u0, o + c * cst, io) = n;
                 en += w * (n.x * n.x + n.y * n.y);
             } else if constexpr (EPI == EPI_CN_MID) {
                 const cplx<T> u = cvt<double2, cplx<T>>(
                     make_double2(0.5 * ((a.x + dt * v[c].x) + a.x), 0.5 * ((a.y + dt * v[c].y) + a.y)));
-                io.us[o + c * cst] = u;
+                BASTR_AT(io.us, o + c * cst, io) = u;
                 if constexpr (NEXT) next[c] = u;
             } else if constexpr (EPI == EPI_CN_LAST) {
                 const double2 n = make_double2(a.x + dt * v[c].x, a.y + dt * v[c].y);
-                io.u0[o + c * cst] = n;
+                BASTR_AT(io.u0, o + c * cst, io) = n;
                 en += w * (n.x * n.x + n.y * n.y);
             }
         }
@@ -339,16 +379,18 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) 
 // Copies `bytes` (a multiple of 8, both ends 8-byte aligned) from global to shared memory with
 // all threads of the block, in 16-byte chunks when both ends and the length allow it and in
 // 8-byte chunks otherwise; returns without waiting.
-__device__ __forceinline__ void stage_line(void* smem_dst, const void* gmem_src, int bytes) {
+// g: the handle's geometry (its check table in the index-checking build).
+__device__ __forceinline__ void stage_line(void* smem_dst, const void* gmem_src, int bytes, const Geo& g) {
     char* d = static_cast<char*>(smem_dst);
     const char* s = static_cast<const char*>(gmem_src);
     if ((((unsigned long long)d | (unsigned long long)s | (unsigned long long)bytes) & 15ull) == 0) {
         const int n16 = bytes >> 4;
-        for (int i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(d + 16 * i, s + 16 * i);
+        for (int i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(d + 16 * i, BASTR_CHK(s + 16 * i, 16, g));
     } else {
         const int n8 = bytes >> 3;
-        for (int i = threadIdx.x; i < n8; i += blockDim.x) cp_async8(d + 8 * i, s + 8 * i);
+        for (int i = threadIdx.x; i < n8; i += blockDim.x) cp_async8(d + 8 * i, BASTR_CHK(s + 8 * i, 8, g));
     }
+    (void)g;
 }
 
 }  // namespace bastr

@@ -112,7 +112,7 @@ cudaError_t rhs2d(bastr_handle* h, int epi, bool from_u0, bool vg) {
         e = l2_xpass<T, XM_RHS>(h, h->ma, ftot, h->mb, nullptr, nullptr, nullptr);
     }
     if (e != cudaSuccess) return e;
-    StageIO<T> io{h->u0, (cplx<T>*)h->us, (cplx<T>*)h->acc, nullptr};
+    StageIO<T> io{h->u0, (cplx<T>*)h->us, (cplx<T>*)h->acc, nullptr, h->g.chk, h->g.err};
     const bool need_en = (epi == EPI_RK3 || epi == EPI_CN_LAST) &&
                          (h->p.forcemethod == 1 || h->p.forcemethod >= 3);
     if (need_en) io.energy_part = h->en_part;

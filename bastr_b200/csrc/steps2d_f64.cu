@@ -9,7 +9,7 @@ template cudaError_t rhs2d<double>(bastr_handle*, int, bool, bool);
 cudaError_t state2d_to_spectral(bastr_handle* h) {
     cudaError_t e = l2_xpass<double, XM_FROM_PHYS>(h, nullptr, 0, h->mb, h->phys, nullptr, nullptr);
     if (e != cudaSuccess) return e;
-    StageIO<double> io{h->u0, nullptr, nullptr, nullptr};
+    StageIO<double> io{h->u0, nullptr, nullptr, nullptr, h->g.chk, h->g.err};
     return l2_yfwd<double, EPI_STORE>(h, h->mb, io, 0);
 }
 

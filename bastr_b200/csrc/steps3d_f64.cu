@@ -11,7 +11,7 @@ cudaError_t state3d_to_spectral(bastr_handle* h) {
     if (e != cudaSuccess) return e;
     e = l3_yfwd<double>(h, h->mc, h->ma);
     if (e != cudaSuccess) return e;
-    StageIO<double> io{h->u0, nullptr, nullptr, nullptr};
+    StageIO<double> io{h->u0, nullptr, nullptr, nullptr, h->g.chk, h->g.err};
     return l3_zfwd<double, EPI_STORE>(h, h->ma, io, 0);
 }
 
