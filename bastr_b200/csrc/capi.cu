@@ -234,6 +234,8 @@ void free_all(bastr_handle* h) {
         if (t.d64) cudaFree(t.d64);
         if (t.d32) cudaFree(t.d32);
     }
+    if (h->stage_dev) cudaFree(h->stage_dev);
+    if (h->stage_host) cudaFreeHost(h->stage_host);
     for (cudaEvent_t ev : h->ev_pool) cudaEventDestroy(ev);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
@@ -628,18 +630,39 @@ int bastr_step_async(bastr_handle* h, int32_t nsteps) {
     return BASTR_OK;
 }
 
+// Gathers a batch's read-back into one contiguous buffer: [stop word, error word] as doubles,
+// then nrec record values, then nsh shell values, so that the host fetches it with one copy.
+__global__ void k_pack_records(const double* __restrict__ rec, const double* __restrict__ shells,
+                               const unsigned int* __restrict__ words, size_t nrec, size_t nsh,
+                               double* __restrict__ out) {
+    const size_t n = 2 + nrec + nsh;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = i < 2 ? (double)words[i] : i < 2 + nrec ? rec[i - 2] : shells[i - 2 - nrec];
+}
+
 int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells) {
     if (!h) return BASTR_E_INVALID;
     if (nsteps < 0 || nsteps > h->chunk_used) return fail(h, BASTR_E_INVALID, "only %d records available", h->chunk_used);
     CK(cudaSetDevice(h->device));
-    std::vector<double> rec((size_t)nsteps * R_COUNT);
-    unsigned int words[2] = {0, 0};   // the batch's stop word and the kernels' error word
-    if (nsteps) CK(cudaMemcpyAsync(rec.data(), h->rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    if (shells && nsteps)
-        CK(cudaMemcpyAsync(shells, h->shells_dev, (size_t)nsteps * 2 * (h->allkmax + 1) * sizeof(double),
-                           cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(words, h->done + T_HALT, sizeof words, cudaMemcpyDeviceToHost, h->stream));
+    // the records, the shells asked for and the batch's two words in one copy into pinned memory
+    const size_t nrec = (size_t)nsteps * R_COUNT;
+    const size_t nsh = shells ? (size_t)nsteps * 2 * (h->allkmax + 1) : 0;
+    const size_t cap = 2 + (size_t)kChunk * (R_COUNT + 2 * (h->allkmax + 1));
+    if (!h->stage_host) {
+        CK(cudaMalloc(&h->stage_dev, cap * sizeof(double)));
+        CK(track_alloc(h, h->stage_dev, cap * sizeof(double)));
+        CK(cudaMallocHost(&h->stage_host, cap * sizeof(double)));
+    }
+    const int grid = (int)std::min<size_t>((2 + nrec + nsh + 255) / 256, 148);
+    k_pack_records<<<grid, 256, 0, h->stream>>>(h->rec, h->shells_dev, h->done + T_HALT, nrec, nsh, h->stage_dev);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->stage_host, h->stage_dev, (2 + nrec + nsh) * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    const double* staged = h->stage_host;
+    const unsigned int words[2] = {(unsigned int)staged[0], (unsigned int)staged[1]};   // stop, error
+    const double* rec = staged + 2;
+    if (shells && nsh) std::memcpy(shells, staged + 2 + nrec, nsh * sizeof(double));
     const unsigned int halt = words[0];
     if (words[1] != 0) {
         CK(cudaMemsetAsync(h->done + T_ERR, 0, sizeof(unsigned int), h->stream));
@@ -651,7 +674,7 @@ int bastr_step_records(bastr_handle* h, int32_t nsteps, bastr_step_out* out, dou
     // the stop word belongs to the last batch (chunk_used steps); a NaN step within the records asked for
     const int valid = apply_halt(h, halt, h->chunk_used);
     const int nv = std::min(valid, (int)nsteps);
-    decode_records(h, rec.data(), nv, out);
+    decode_records(h, rec, nv, out);
     if (nv < nsteps) {
         blank_records(out, nv, nsteps);
         if (shells)

@@ -94,6 +94,10 @@ struct bastr_handle {
     double* shell = nullptr;   // [nshell][4]
     double* rec = nullptr;     // [kChunk][R_COUNT]
     double* shells_dev = nullptr; // [kChunk][2][allkmax+1]
+    // read-back of a batch in one copy (bastr_step_records): device gather buffer and pinned
+    // host copy, [2 words + kChunk records + kChunk shell pairs]; allocated on first use
+    double* stage_dev = nullptr;
+    double* stage_host = nullptr;
     int64_t dev_bytes = 0;
     size_t n_state = 0;        // complex entries of the truncated state (all components)
     int n_vg_blocks = 0;
