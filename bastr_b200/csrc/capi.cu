@@ -226,7 +226,7 @@ template <typename P> void dev_alloc(bastr_handle* h, P** ptr, size_t bytes, cud
 void free_all(bastr_handle* h) {
     void* ptrs[] = {h->u0, h->us, h->acc, h->ma, h->mb, h->mc, h->phys, h->vg_part, h->en_part, h->done, h->pend, h->rng, h->closure_buf, h->tr_buf, h->tr_modes, h->hg_part,
                     h->sg_buf, h->sg_tw,
-                    h->shell, h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
+                    h->rec, h->shells_dev, h->sp_modes, h->sp_item_lo, h->sp_shell_item,
                     h->sp_item_part, h->chk_table};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -347,7 +347,6 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
     dev_alloc(h, &h->rng, sizeof(unsigned long long), st);
     dev_alloc(h, &h->vg_part, (size_t)std::max(g.ny * g.nz, 1) * 8 * sizeof(double), st);
     dev_alloc(h, &h->en_part, (size_t)std::max(K * g.KY, 1) * sizeof(double), st);
-    dev_alloc(h, &h->shell, (size_t)h->nshell * 4 * sizeof(double), st);
     dev_alloc(h, &h->rec, (size_t)kChunk * R_COUNT * sizeof(double), st);
     dev_alloc(h, &h->shells_dev, (size_t)kChunk * 2 * (h->allkmax + 1) * sizeof(double), st);
     if (st != cudaSuccess) return fail(h, BASTR_E_CUDA, "device allocation failed: %s", cudaGetErrorString(st));
@@ -435,7 +434,7 @@ int bastr_create(const bastr_params* p, bastr_handle** out) {
         std::vector<int> fill(cnt.begin(), cnt.end() - 1);
         each_mode([&](int idx, int sh) { modes[fill[sh]++] = idx; });
         h->n_disk = modes.size() + 1;   // plus the k = 0 mode
-        constexpr int kItem = 2048;     // list entries per work item
+        constexpr int kItem = BASTR_SPECTRA_ITEM;   // list entries per work item
         std::vector<int> item_lo, shell_item(h->nshell + 1, 0);
         for (int sh = 0; sh < h->nshell; ++sh) {
             shell_item[sh] = (int)item_lo.size();

@@ -19,6 +19,10 @@
 #ifndef BASTR_SPECTRA_U
 #define BASTR_SPECTRA_U 4
 #endif
+// List entries of one work item (one block) of the spectra kernel.
+#ifndef BASTR_SPECTRA_ITEM
+#define BASTR_SPECTRA_ITEM 2048
+#endif
 
 namespace bastr {
 

@@ -91,7 +91,6 @@ struct bastr_handle {
     double2* pend = nullptr;       // (pending, factor) of a linear-forcing scale not yet applied
     unsigned long long* rng = nullptr;  // forcing calls so far: counter of the random-phase stream
     bool scale_pending = false;    // host view: a step with linear forcing ran since the last spectra
-    double* shell = nullptr;   // [nshell][4]
     double* rec = nullptr;     // [kChunk][R_COUNT]
     double* shells_dev = nullptr; // [kChunk][2][allkmax+1]
     // read-back of a batch in one copy (bastr_step_records): device gather buffer and pinned
