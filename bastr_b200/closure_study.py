@@ -89,7 +89,8 @@ def run(args) -> dict:
     cur = torch.cuda.current_stream()
     hist, t_train = _device_ms(cur, lambda: net.train(train, iters=args.iters, lr=args.lr))
 
-    # 3. test: the held-out fine run (the judge), and two coarse runs from its filtered field
+    # 3. test: the held-out fine run (the reference solution), and two coarse runs from its
+    # filtered field
     def coarse_spectrum(fields):
         with BastrGPU(nc, nc, nc, **phys) as c:
             c.set_state(fields)
