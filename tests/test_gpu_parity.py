@@ -69,6 +69,23 @@ def test_2d_nonsquare(gpu_lib):
     _check(err, 1e-10)
 
 
+@pytest.mark.parametrize("dims,kw", [
+    ((32, 128, 0), dict(reynolds=2000.0, deltat=1e-4, timemethod=2, forcemethod=1, target_energy=1.0)),
+    ((128, 256, 0), dict(reynolds=5000.0, deltat=1e-4, forcemethod=5, forcek=4, target_energy=1.5, lprojectd=True)),
+], ids=["32x128_cn_linear", "128x256_band5_proj"])
+def test_2d_nonsquare_forms(gpu_lib, dims, kw):
+    """More non-square 2D grids: Crank-Nicolson with linear forcing and RK3 with projected band
+    forcing; FP64 over 10 steps at 1e-9 and the FP32 form at 1e-5."""
+    ia, ja, ka = dims
+    p = make_params(ia, ja, ka, **kw)
+    u = field(ia, ja, ka, k0=3.0, seed=8)
+    ref = run_oracle(p, u, 10)
+    _check(compare(ref, run_gpu(p, u, 10, "fp64")), 1e-9)
+    err = compare(ref, run_gpu(p, u, 10, "fp32"))
+    _check({k: v for k, v in err.items() if k != "eta_min"}, 1e-5)
+    assert err["eta_min"] <= 1e-4
+
+
 def test_2d_512_hundred_steps(gpu_lib):
     """The 512^2 decaying configuration (Re 5000, dt 1e-4, spectra to kmax 170), 100 steps."""
     p = make_params(512, 512, 0, reynolds=5000.0, deltat=1e-4, kmax=170)
@@ -100,6 +117,25 @@ def test_3d_fp64_many_steps(gpu_lib, name, kw, k0):
     u = field(32, 32, 32, k0=k0, seed=5)
     err = compare(run_oracle(p, u, 20), run_gpu(p, u, 20, "fp64"))
     _check(err, 1e-9)
+
+
+@pytest.mark.parametrize("dims,kw", [
+    ((32, 64, 32), dict(reynolds=2000.0, deltat=5e-4, forcemethod=2, forcek=3, target_energy=0.2, lprojectd=True)),
+    ((32, 32, 64), dict(reynolds=2000.0, deltat=5e-4, forcemethod=1, target_energy=1.5)),
+    ((16, 32, 64), dict(reynolds=1000.0, deltat=5e-4, timemethod=2, forcemethod=5, forcek=2, target_energy=2.0)),
+], ids=["32x64x32_band_proj", "32x32x64_linear", "16x32x64_cn_band5"])
+def test_3d_noncubic(gpu_lib, dims, kw):
+    """Grids whose three extents differ (ja, ka >= 2*floor(ia/3)): the truncated layout keeps
+    2K-1 modes along y and z whatever ja and ka are, and the passes transform ja and ka points.
+    FP64 over 10 steps at 1e-9, the FP32 form at 1e-5."""
+    ia, ja, ka = dims
+    p = make_params(ia, ja, ka, **kw)
+    u = field(ia, ja, ka, k0=3.0, seed=7)
+    ref = run_oracle(p, u, 10)
+    _check(compare(ref, run_gpu(p, u, 10, "fp64")), 1e-9)
+    err = compare(ref, run_gpu(p, u, 10, "fp32"))
+    _check({k: v for k, v in err.items() if k != "eta_min"}, 1e-5)
+    assert err["eta_min"] <= 1e-4
 
 
 def test_3d_64_ten_steps(gpu_lib):
