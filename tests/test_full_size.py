@@ -21,6 +21,8 @@ W2D = dict(ia=2048, ja=2048, ka=0, reynolds=5000.0, deltat=1e-4, forcemethod=2, 
            lprojectd=True, kmax=1 << 30)
 W3D = dict(ia=256, ja=256, ka=256, reynolds=5000.0, deltat=5e-4, forcemethod=1, forcek=5, target_energy=1.5,
            lprojectd=False, kmax=85)
+# the largest 3D grid the library builds (extents up to 512)
+W3D512 = dict(W3D, ia=512, ja=512, ka=512, deltat=2.5e-4, kmax=170)
 
 
 def _params(w):
@@ -41,7 +43,8 @@ def test_2d2048_fp64_one_step_matches_oracle(gpu_lib):
     _check(compare(run_oracle(p, u, 1), run_gpu(p, u, 1, "fp64")), 1e-12)
 
 
-@pytest.mark.parametrize("w,nsteps", [(W2D, 100), (W3D, 100)], ids=["2d2048_100", "3d256_100"])
+@pytest.mark.parametrize("w,nsteps", [(W2D, 100), (W3D, 100), (W3D512, 20)],
+                         ids=["2d2048_100", "3d256_100", "3d512_20"])
 def test_fp32_form_against_fp64_form(gpu_lib, w, nsteps):
     """The FP32 form's error against the FP64 form at the measured size.  eta_min is a pointwise
     extremum of sqrt(nu/|div|), so FP32 round-off of one point enters it unsmoothed: 1e-4."""
