@@ -138,6 +138,26 @@ def test_3d_noncubic(gpu_lib, dims, kw):
     assert err["eta_min"] <= 1e-4
 
 
+@pytest.mark.parametrize("dims,kw", [
+    ((16, 16, 0), dict(reynolds=1000.0, deltat=2e-4, forcemethod=2, forcek=2, target_energy=0.1, lprojectd=True)),
+    ((32, 32, 0), dict(reynolds=1000.0, deltat=2e-4, timemethod=2, forcemethod=1, target_energy=1.0)),
+    ((16, 16, 16), dict(reynolds=1000.0, deltat=5e-4, forcemethod=5, forcek=2, target_energy=2.0)),
+    ((16, 16, 32), dict(reynolds=1000.0, deltat=5e-4, timemethod=2, lprojectd=True)),
+], ids=["16x16_band_proj", "32x32_cn_linear", "16x16x16_band5", "16x16x32_cn_proj"])
+def test_smallest_grids(gpu_lib, dims, kw):
+    """The smallest extents the library builds (16 points: K = 5, transforms of 16 points), where
+    every line holds few modes and most lanes of a line group are idle; FP64 over 10 steps at
+    1e-9 and the FP32 form at 1e-5."""
+    ia, ja, ka = dims
+    p = make_params(ia, ja, ka, **kw)
+    u = field(ia, ja, ka, k0=2.0, seed=9)
+    ref = run_oracle(p, u, 10)
+    _check(compare(ref, run_gpu(p, u, 10, "fp64")), 1e-9)
+    err = compare(ref, run_gpu(p, u, 10, "fp32"))
+    _check({k: v for k, v in err.items() if k != "eta_min"}, 1e-5)
+    assert err["eta_min"] <= 1e-4
+
+
 def test_3d_64_ten_steps(gpu_lib):
     p = make_params(64, 64, 64, reynolds=5000.0, deltat=5e-4, forcemethod=1, target_energy=1.5, kmax=21)
     u = field(64, 64, 64, k0=3.0, seed=0)
