@@ -158,6 +158,35 @@ def test_smallest_grids(gpu_lib, dims, kw):
     assert err["eta_min"] <= 1e-4
 
 
+@pytest.mark.parametrize("dims,every", [((64, 64, 0), 3), ((32, 32, 32), 2)], ids=["2d_every3", "3d_every2"])
+def test_velgrad_every_n_steps(gpu_lib, dims, every):
+    """Statistics every n steps (velgrad_every = n; the reference computes them every step): the
+    steps with nstep % n == 0 carry the oracle's eight statistics, the others NaN, and the
+    dynamics (state, spectra, forcing) are those of the every-step run."""
+    import numpy as np
+    from bastr_b200 import BastrGPU
+    from tests.parity_util import rel_l2
+    ia, ja, ka = dims
+    kw = dict(reynolds=2000.0, deltat=2e-4 if ka == 0 else 5e-4, forcemethod=2, forcek=3, target_energy=0.2)
+    p = make_params(ia, ja, ka, **kw)
+    u = field(ia, ja, ka, k0=3.0, seed=10)
+    rrec, rsh, ru = run_oracle(p, u, 7)
+    with BastrGPU(ia, ja, ka, precision="fp64", velgrad_every=every, **kw) as s:
+        s.set_state(u)
+        recs, shells = s.step(7, shells=True)
+        ug = s.get_state()
+    assert rel_l2(np.stack(ug), np.stack(ru)) <= 1e-10
+    for name in ("Esspe", "Edspe", "factor"):
+        got = [getattr(r, name) for r in recs]
+        want = [getattr(r, name) if name != "factor" else r.forcing[0] for r in rrec]
+        assert rel_l2(got, want) <= 1e-10, name
+    for i, (g, r) in enumerate(zip(recs, rrec)):
+        if i % every == 0:
+            assert rel_l2(g.velgrad, r.velgrad) <= 1e-10, i
+        else:
+            assert all(np.isnan(v) for v in g.velgrad), i
+
+
 def test_3d_64_ten_steps(gpu_lib):
     p = make_params(64, 64, 64, reynolds=5000.0, deltat=5e-4, forcemethod=1, target_energy=1.5, kmax=21)
     u = field(64, 64, 64, k0=3.0, seed=0)
