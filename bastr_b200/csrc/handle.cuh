@@ -326,9 +326,14 @@ cudaError_t launch_k(bastr_handle* h, void (*kernel)(KArgs...), dim3 grid, dim3 
 }
 
 // Enables the dynamic shared memory a kernel instance asks for and returns how many of its
-// blocks fit on one SM; both once per (device, kernel).
+// blocks fit on one SM.  The shared-memory limit is an attribute of the kernel, not of one
+// launch size, and some kernels ask for a size that depends on the grid (the 3D y-forward pass's
+// tile follows KY): the limit set per (device, kernel) only ever grows, so a smaller request
+// never lowers it under a larger one made before.  Occupancy is cached per (device, kernel,
+// size).
 inline std::mutex g_prep_mu;
 inline std::map<std::tuple<int, const void*, size_t>, int> g_prepped;
+inline std::map<std::pair<int, const void*>, size_t> g_smem_limit;
 inline int g_num_sms[64] = {};
 template <typename K> cudaError_t prep(K kernel, size_t smem, int nt = 0, int* blocks_per_sm = nullptr) {
     int dev = 0;
@@ -336,12 +341,16 @@ template <typename K> cudaError_t prep(K kernel, size_t smem, int nt = 0, int* b
     if (e != cudaSuccess) return e;
     const auto key = std::make_tuple(dev, (const void*)kernel, smem);
     std::lock_guard<std::mutex> lk(g_prep_mu);
-    auto it = g_prepped.find(key);
-    if (it == g_prepped.end()) {
-        if (smem > 48 * 1024) {
+    if (smem > 48 * 1024) {
+        size_t& limit = g_smem_limit[std::make_pair(dev, (const void*)kernel)];
+        if (smem > limit) {
             e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
+            limit = smem;
         }
+    }
+    auto it = g_prepped.find(key);
+    if (it == g_prepped.end()) {
         int nb = 1;
         if (nt > 0) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, nt, smem);

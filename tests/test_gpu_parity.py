@@ -158,6 +158,20 @@ def test_smallest_grids(gpu_lib, dims, kw):
     assert err["eta_min"] <= 1e-4
 
 
+def test_kernel_shared_memory_limit_never_shrinks(gpu_lib):
+    """Grids with the same ja share the 3D y-forward kernel instance, whose shared memory follows
+    KY: a 32^3 handle, then a 16x32x64 one (smaller KY, smaller request), then 32^3 again must
+    all run (the kernel's shared-memory limit is set per kernel and must not drop under the
+    first, larger request)."""
+    import numpy as np
+    from bastr_b200 import BastrGPU
+    for dims in ((32, 32, 32), (16, 32, 64), (32, 32, 32)):
+        with BastrGPU(*dims, precision="fp64", velgrad_every=1) as s:
+            s.set_state(field(*dims, k0=3.0, seed=1))
+            recs = s.step(2)
+            assert np.isfinite(recs[-1].Esspe)
+
+
 @pytest.mark.parametrize("dims,every", [((64, 64, 0), 3), ((32, 32, 32), 2)], ids=["2d_every3", "3d_every2"])
 def test_velgrad_every_n_steps(gpu_lib, dims, every):
     """Statistics every n steps (velgrad_every = n; the reference computes them every step): the
