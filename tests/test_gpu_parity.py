@@ -172,6 +172,40 @@ def test_kernel_shared_memory_limit_never_shrinks(gpu_lib):
             assert np.isfinite(recs[-1].Esspe)
 
 
+def test_interleaved_handles_match_solo_runs(gpu_lib):
+    """Handles of different shapes and forms alive at once, stepped in turn on their own streams
+    (they share kernel instances, launch caches and twiddle tables): every handle's records and
+    state are bitwise those of the same handle run alone."""
+    import numpy as np
+    from bastr_b200 import BastrGPU
+    cases = [((32, 32, 32), "fp64"), ((16, 32, 64), "fp64"), ((64, 128, 0), "fp32"), ((32, 32, 32), "fp32")]
+    kw = dict(reynolds=2000.0, deltat=5e-4, forcemethod=2, forcek=2, target_energy=0.3, velgrad_every=1)
+
+    def values(recs, state):
+        return np.concatenate([np.array([[r.Esspe, r.Edspe, r.factor, *r.velgrad] for r in recs]).ravel(),
+                               np.stack(state).ravel()])
+
+    solo = []
+    for dims, prec in cases:
+        with BastrGPU(*dims, precision=prec, **kw) as s:
+            s.set_state(field(*dims, k0=3.0, seed=2))
+            recs = s.step(3) + s.step(3)
+            solo.append(values(recs, s.get_state()))
+    handles = [BastrGPU(*dims, precision=prec, **kw) for dims, prec in cases]
+    try:
+        for (dims, _), s in zip(cases, handles):
+            s.set_state(field(*dims, k0=3.0, seed=2))
+        recs = [[] for _ in cases]
+        for _ in range(2):
+            for i, s in enumerate(handles):
+                recs[i] += s.step(3)
+        for i, s in enumerate(handles):
+            assert np.array_equal(values(recs[i], s.get_state()), solo[i]), cases[i]
+    finally:
+        for s in handles:
+            s.close()
+
+
 @pytest.mark.parametrize("dims,every", [((64, 64, 0), 3), ((32, 32, 32), 2)], ids=["2d_every3", "3d_every2"])
 def test_velgrad_every_n_steps(gpu_lib, dims, every):
     """Statistics every n steps (velgrad_every = n; the reference computes them every step): the
