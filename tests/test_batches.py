@@ -52,3 +52,29 @@ def test_zero_steps_runs_nothing(gpu_lib):
         assert recs == [] and shells.shape[0] == 0
         assert s.counters() == (0, 0.0)
         assert np.array_equal(np.stack(s.get_state()), before)
+
+
+@pytest.mark.parametrize("dims,method", [((64, 64, 0), 3), ((16, 16, 16), 4)], ids=["2d_m3", "3d_m4"])
+def test_restart_continues_the_run(gpu_lib, dims, method):
+    """A restart (the reference's read_continue_field, then the main loop from the saved nstep):
+    a new handle given the state and counters after 5 steps continues the run, random-phase forcing
+    included (its phases follow the step counter), within 1e-11 of the uninterrupted run; the
+    state passes through its physical form once, hence not bitwise."""
+    from bastr_b200 import BastrGPU
+    from tests.parity_util import rel_l2
+    kw = dict(KW, forcemethod=method, forcek=2, target_energy=0.2 if method == 3 else 0.05)
+    u = field(*dims, k0=3.0, seed=14)
+    with BastrGPU(*dims, precision="fp64", **kw) as a:
+        a.set_state(u)
+        a.step(5)
+        mid, (n5, t5) = a.get_state(), a.counters()
+        tail = a.step(5)
+        end = np.stack(a.get_state())
+    with BastrGPU(*dims, precision="fp64", **kw) as b:
+        b.set_state(mid)
+        b.set_counters(n5, t5)
+        again = b.step(5)
+        assert [r.nstep for r in again] == [r.nstep for r in tail]
+        assert [r.time for r in again] == [r.time for r in tail]
+        assert rel_l2(_values(again)[:, 2:], _values(tail)[:, 2:]) <= 1e-11
+        assert rel_l2(np.stack(b.get_state()), end) <= 1e-11
