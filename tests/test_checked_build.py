@@ -8,9 +8,10 @@ registered buffer.  An access that does not sets a bit in the handle's error wor
 scratch line instead (no fault), and the next ``bastr_step`` returns BASTR_E_CUDA.  The tensor
 maps of the TMA staging are checked against the buffers at creation in every build.
 
-CPU: the checked library exports the same entry points as the normal one.  GPU: the small
-cases of tests/checked_cases.py (2D and 3D, square and not, FP64 and FP32, RK3 and
-Crank-Nicolson, forcing methods 1-5, statistics every step, spectra and transfer spectra) run
+CPU: the checked library exports the same entry points as the normal one.  GPU: the cases of
+tests/checked_cases.py (2D and 3D, square and not, FP64 and FP32, RK3 and Crank-Nicolson, forcing
+methods 1-5, statistics every step, spectra and transfer spectra, and the measured sizes 2048^2
+and 256^3) run
 through both libraries in separate processes: the checked run reports no bad access, and its
 results are bitwise those of the normal build (the checks never change an in-bounds access).
 """
