@@ -91,3 +91,34 @@ def test_checked_build_reports_a_planted_table_error(precision):
             assert out.startswith(f"code {BASTR_E_CUDA}") and "index check" in out, out
         else:
             assert out == "no error", out
+
+
+def _calls(text, name):
+    """The argument text of every call `name(...)` in `text` (balanced parentheses)."""
+    out, i = [], 0
+    while True:
+        j = text.find(name + "(", i)
+        if j < 0:
+            return out
+        k, depth = j + len(name) + 1, 1
+        while depth:
+            depth += {"(": 1, ")": -1}.get(text[k], 0)
+            k += 1
+        out.append(text[j + len(name) + 1:k - 1])
+        i = k
+
+
+def test_pass_kernels_route_their_global_accesses_through_the_checks():
+    """Source guard for the checked build's coverage: in the pass kernels every cp.async source,
+    every line staging and every paired vector store goes through BASTR_CHK (or passes the
+    geometry that carries the table), so a new access of these kinds cannot skip the checker."""
+    csrc = os.path.join(ROOT, "bastr_b200", "csrc")
+    for fname in ("pass2d.cu", "pass3d.cu"):
+        text = open(os.path.join(csrc, fname)).read()
+        for name in ("cp_async16", "cp_async8"):
+            for args in _calls(text, name):
+                assert "BASTR_CHK" in args, (fname, name, args)
+        for args in _calls(text, "stage_line"):
+            assert args.rstrip().endswith(", g"), (fname, args)
+        for args in _calls(text, "st2<T>"):
+            assert args.lstrip().startswith("BASTR_CHK("), (fname, args)
