@@ -103,7 +103,9 @@ BASTR_API int bastr_get_counters(bastr_handle* h, int64_t* nstep, double* time);
  * as the reference stops there (solution.F90:69-81), also when out is NULL: that step's record is
  * filled, the records and shells of the later steps are NaN, no kernel of a later step runs, and
  * the state and the counters (bastr_get_state, bastr_get_counters) are those of the NaN step, the
- * state the reference dumps before it stops. */
+ * state the reference dumps before it stops.  Returns BASTR_E_CUDA, with a message, when a kernel
+ * of the batch reported an internal error instead of faulting: a bounded wait for its TMA staging
+ * that gave up, or (libbastr_gpu_checked.so) an access outside the handle's buffers. */
 BASTR_API int bastr_step(bastr_handle* h, int32_t nsteps, bastr_step_out* out, double* shells);
 
 /* Enqueues nsteps iterations on the handle's stream and returns without synchronising;
